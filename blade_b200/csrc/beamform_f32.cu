@@ -1,0 +1,393 @@
+// Plain FP32 CUDA-core beamformer (the drop-in) and the fused FP32 chain
+// Cast -> Beamformer -> Channelizer(rate 1|2|4) -> Detector (Stokes-I).
+//
+// Reference: src/modules/beamformer/beamformer.cu:13-79.  There one thread owns one
+// time sample, caches all A x P antenna samples in registers and loops over beams
+// with the phasors in a static [B][A][P] shared array (so B x A x P is capped by
+// the 48 KB static limit, and A = B = 64 does not compile) and the block size is
+// capped by the register file at large A.
+//
+// Here a CTA owns one channel f, a tile of TT = 4 TG consecutive time samples and
+// a tile of BT = 4 (256 / TG) beams.  Thread (tg, bg) accumulates a 4 x 4 register
+// tile: 4 consecutive time samples x 4 beams x P polarisations.  Antennas stream
+// through double-buffered shared memory in chunks of AC = 256 / TG (voltages stored
+// time-interleaved so that the per-thread 4-sample reads are bank-conflict free;
+// phasors read as broadcasts); the next chunk's global loads are in flight while
+// the current chunk is multiplied.  Any A, B, F, T.
+//
+// The fused chain keeps the beam voltages in registers: the 4 consecutive samples
+// of a thread are one rate-4 spectrum (or two rate-2 spectra, or four rate-1
+// samples); the (-1)^t fftshift pre-multiply and the DFT are applied in
+// registers (their coefficients are +-1, +-i), |.|^2 is summed over both
+// polarisations, and the integration window is closed with warp shuffles over
+// adjacent lanes.  Nothing but the Stokes-I output touches HBM.
+#include "common.cuh"
+
+namespace bb {
+namespace {
+
+enum { IN_CF32 = 0, IN_CI8 = 1 };
+
+__device__ __forceinline__ void cmac(float2& acc, float2 x, float2 w) {
+    acc.x = fmaf(x.x, w.x, acc.x);
+    acc.x = fmaf(-x.y, w.y, acc.x);
+    acc.y = fmaf(x.x, w.y, acc.y);
+    acc.y = fmaf(x.y, w.x, acc.y);
+}
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmuli(float2 a) { return make_float2(-a.y, a.x); }  // i * a
+__device__ __forceinline__ float pw(float2 a) { return a.x * a.x + a.y * a.y; }
+
+template <int P, int TG, int IN, int R>
+__global__ void __launch_bounds__(256, 2) bf32_kernel(const void* __restrict__ vin, const float2* __restrict__ phasors,
+                                                   void* __restrict__ vout, uint32_t B, uint32_t A, uint32_t F,
+                                                   uint32_t T, uint32_t integ) {
+    constexpr int BGN = 256 / TG;
+    constexpr int BT = BGN * 4;
+    constexpr int TT = TG * 4;
+    constexpr int AC = 256 / TG;
+    constexpr int XPT = 4;  // samples loaded per thread per chunk: AC * TT / 256 = 4
+    static_assert(AC * TT == 1024, "chunk must hold 1024 samples");
+
+    __shared__ __align__(16) float2 xs[2][AC][4][TG][P];
+    __shared__ __align__(16) float2 ws[2][AC][BT][P];
+
+    const int tid = threadIdx.x;
+    const int tg = tid % TG, bg = tid / TG;
+    const uint32_t t0 = blockIdx.x * TT;
+    const uint32_t f = blockIdx.y;
+    const uint32_t b0 = blockIdx.z * BT;
+
+    // Prefetch registers.
+    float2 xr[XPT][P];
+    float2 wr[2];
+
+    auto load_chunk = [&](uint32_t a0) {
+#pragma unroll
+        for (int m = 0; m < XPT; m++) {
+            const int s = tid + 256 * m;
+            const int al = s / TT, tl = s % TT;
+            const uint32_t a = a0 + al, t = t0 + tl;
+            if (a < A && t < T) {
+                const uint64_t idx = ((uint64_t)(a * (uint64_t)F + f) * T + t) * P;
+                if (IN == IN_CF32) {
+                    const float2* x = static_cast<const float2*>(vin) + idx;
+                    if (P == 2) {
+                        float4 v = ldg_nc_f4(x);
+                        xr[m][0] = make_float2(v.x, v.y);
+                        xr[m][P - 1] = make_float2(v.z, v.w);
+                    } else {
+                        xr[m][0] = __ldg(x);
+                    }
+                } else {
+                    const char2* x = static_cast<const char2*>(vin) + idx;
+                    if (P == 2) {
+                        char4 v = __ldg(reinterpret_cast<const char4*>(x));
+                        xr[m][0] = make_float2((float)v.x, (float)v.y);
+                        xr[m][P - 1] = make_float2((float)v.z, (float)v.w);
+                    } else {
+                        char2 v = __ldg(x);
+                        xr[m][0] = make_float2((float)v.x, (float)v.y);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int p = 0; p < P; p++) xr[m][p] = make_float2(0.f, 0.f);
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+            const int e = tid + 256 * m;  // over AC * BT * P elements (<= 512)
+            wr[m] = make_float2(0.f, 0.f);
+            if (e < AC * BT * P) {
+                const int p = e % P, j = (e / P) % BT, al = e / (P * BT);
+                const uint32_t a = a0 + al, b = b0 + j;
+                if (a < A && b < B) wr[m] = __ldg(phasors + ((uint64_t)(b * (uint64_t)A + a) * F + f) * P + p);
+            }
+        }
+    };
+    auto store_chunk = [&](int buf) {
+#pragma unroll
+        for (int m = 0; m < XPT; m++) {
+            const int s = tid + 256 * m;
+            const int al = s / TT, tl = s % TT;
+#pragma unroll
+            for (int p = 0; p < P; p++) xs[buf][al][tl % 4][tl / 4][p] = xr[m][p];
+        }
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+            const int e = tid + 256 * m;
+            if (e < AC * BT * P) {
+                const int p = e % P, j = (e / P) % BT, al = e / (P * BT);
+                ws[buf][al][j][p] = wr[m];
+            }
+        }
+    };
+
+    float2 acc[4][4][P];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int p = 0; p < P; p++) acc[i][j][p] = make_float2(0.f, 0.f);
+
+    const uint32_t nchunks = (A + AC - 1) / AC;
+    load_chunk(0);
+    store_chunk(0);
+    __syncthreads();
+    for (uint32_t c = 0; c < nchunks; c++) {
+        const int buf = c & 1;
+        if (c + 1 < nchunks) load_chunk((c + 1) * AC);
+#pragma unroll
+        for (int al = 0; al < AC; al++) {
+            float2 xv[4][P], wv[4][P];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                if (P == 2) {
+                    float4 v = *reinterpret_cast<const float4*>(&xs[buf][al][i][tg][0]);
+                    xv[i][0] = make_float2(v.x, v.y);
+                    xv[i][P - 1] = make_float2(v.z, v.w);
+                } else {
+                    xv[i][0] = xs[buf][al][i][tg][0];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (P == 2) {
+                    float4 v = *reinterpret_cast<const float4*>(&ws[buf][al][bg * 4 + j][0]);
+                    wv[j][0] = make_float2(v.x, v.y);
+                    wv[j][P - 1] = make_float2(v.z, v.w);
+                } else {
+                    wv[j][0] = ws[buf][al][bg * 4 + j][0];
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+#pragma unroll
+                    for (int p = 0; p < P; p++) cmac(acc[i][j][p], xv[i][p], wv[j][p]);
+        }
+        if (c + 1 < nchunks) store_chunk(buf ^ 1);
+        __syncthreads();
+    }
+
+    const uint32_t tb = t0 + tg * 4;  // first of this thread's 4 samples
+    if constexpr (R == 0) {
+        // Beam voltages, CF32 [B, F, T, P].
+        float2* out = static_cast<float2*>(vout);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const uint32_t b = b0 + bg * 4 + j;
+            if (b >= B) continue;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint32_t t = tb + i;
+                if (t >= T) continue;
+                float2* o = out + ((uint64_t)(b * (uint64_t)F + f) * T + t) * P;
+                if (P == 2) stg_f4(o, make_float4(acc[i][j][0].x, acc[i][j][0].y, acc[i][j][P - 1].x,
+                                                  acc[i][j][P - 1].y));
+                else o[0] = acc[i][j][0];
+            }
+        }
+    } else {
+        // Stokes-I of the rate-R channelized beams, integrated over `integ` spectra.
+        constexpr int NS = 4 / R;  // spectra held by this thread
+        float* out = static_cast<float*>(vout);
+        const uint32_t U = T / (R * integ);
+        const uint32_t s0 = tb / R;  // first spectrum index of this thread
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const uint32_t b = b0 + bg * 4 + j;
+            float S[NS][R];
+#pragma unroll
+            for (int q = 0; q < NS; q++) {
+#pragma unroll
+                for (int k = 0; k < R; k++) S[q][k] = 0.f;
+#pragma unroll
+                for (int p = 0; p < P; p++) {
+                    if (R == 1) {
+                        S[q][0] += pw(acc[q][j][p]);
+                    } else if (R == 2) {
+                        const float2 y0 = acc[2 * q][j][p], y1 = acc[2 * q + 1][j][p];
+                        S[q][0] += pw(csub(y0, y1));
+                        S[q][R - 1] += pw(cadd(y0, y1));
+                    } else {
+                        const float2 y0 = acc[0][j][p], y1 = acc[1][j][p], y2 = acc[2][j][p], y3 = acc[3][j][p];
+                        const float2 e02 = cadd(y0, y2), d02 = csub(y0, y2);
+                        const float2 e13 = cadd(y1, y3), d13 = csub(y1, y3);
+                        S[q][0] += pw(csub(e02, e13));                 // y0 - y1 + y2 - y3
+                        S[q][R > 1 ? 1 : 0] += pw(cadd(d02, cmuli(d13)));  // y0 + i y1 - y2 - i y3
+                        S[q][R > 2 ? 2 : 0] += pw(cadd(e02, e13));     // y0 + y1 + y2 + y3
+                        S[q][R > 3 ? 3 : 0] += pw(csub(d02, cmuli(d13)));  // y0 - i y1 - y2 + i y3
+                    }
+                }
+            }
+            if ((uint32_t)NS >= integ) {
+                // Whole windows inside the thread.
+                const uint32_t nw = NS / integ;
+                for (uint32_t v = 0; v < nw; v++) {
+#pragma unroll
+                    for (int k = 0; k < R; k++) {
+                        float sum = 0.f;
+                        for (uint32_t q = v * integ; q < (v + 1) * integ; q++) sum += S[q][k];
+                        const uint32_t u = s0 / integ + v;
+                        if (b < B && u < U) out[((uint64_t)(b * (uint64_t)F + f) * R + k) * U + u] = sum;
+                    }
+                }
+            } else {
+                // Window spans g = integ / NS adjacent lanes (power of two <= 32).
+                const uint32_t g = integ / NS;
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    float sum = 0.f;
+#pragma unroll
+                    for (int q = 0; q < NS; q++) sum += S[q][k];
+                    for (uint32_t o = 1; o < g; o <<= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+                    const uint32_t u = s0 / integ;
+                    if ((tg % g) == 0 && b < B && u < U) out[((uint64_t)(b * (uint64_t)F + f) * R + k) * U + u] = sum;
+                }
+            }
+        }
+    }
+}
+
+// Incoherent beam: out[B, f, t, p] = ([sqrt] sum_a |x[a,f,t,p] w[0,a,f,0,p]|^2, 0)
+// (reference src/modules/beamformer/beamformer.cu:64-78).
+template <int P>
+__global__ void __launch_bounds__(256) incoherent_kernel(const float2* __restrict__ in,
+                                                         const float2* __restrict__ phasors, float2* __restrict__ out,
+                                                         uint32_t B, uint32_t A, uint32_t F, uint32_t T, int do_sqrt) {
+    const uint64_t n = (uint64_t)F * T;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t f = i / T;
+        float acc[P];
+#pragma unroll
+        for (int p = 0; p < P; p++) acc[p] = 0.f;
+        for (uint32_t a = 0; a < A; a++) {
+#pragma unroll
+            for (int p = 0; p < P; p++) {
+                const float2 x = in[((uint64_t)a * F * T + i) * P + p];
+                const float2 w = phasors[((uint64_t)a * F + f) * P + p];
+                const float re = x.x * w.x - x.y * w.y, im = x.x * w.y + x.y * w.x;
+                acc[p] += re * re + im * im;
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < P; p++)
+            out[((uint64_t)B * F * T + i) * P + p] = make_float2(do_sqrt ? sqrtf(acc[p]) : acc[p], 0.f);
+    }
+}
+
+template <int P, int TG, int IN, int R>
+void launch_bf(const void* in, const float2* ph, void* out, uint64_t B, uint64_t A, uint64_t F, uint64_t T,
+               uint64_t integ, cudaStream_t s) {
+    constexpr int TT = TG * 4, BT = (256 / TG) * 4;
+    dim3 grid((unsigned)ceil_div(T, TT), (unsigned)F, (unsigned)ceil_div(B, BT));
+    bf32_kernel<P, TG, IN, R><<<grid, 256, 0, s>>>(in, ph, out, (uint32_t)B, (uint32_t)A, (uint32_t)F, (uint32_t)T,
+                                                   (uint32_t)integ);
+}
+
+int pick_tg(uint64_t B) { return B <= 4 ? 256 : B <= 8 ? 128 : B <= 16 ? 64 : 32; }
+
+template <int P, int IN, int R>
+void dispatch_tg(int tg, const void* in, const float2* ph, void* out, uint64_t B, uint64_t A, uint64_t F, uint64_t T,
+                 uint64_t integ, cudaStream_t s) {
+    switch (tg) {
+        case 256: launch_bf<P, 256, IN, R>(in, ph, out, B, A, F, T, integ, s); break;
+        case 128: launch_bf<P, 128, IN, R>(in, ph, out, B, A, F, T, integ, s); break;
+        case 64: launch_bf<P, 64, IN, R>(in, ph, out, B, A, F, T, integ, s); break;
+        default: launch_bf<P, 32, IN, R>(in, ph, out, B, A, F, T, integ, s); break;
+    }
+}
+
+bool dims_ok(uint64_t B, uint64_t A, uint64_t F, uint64_t T) {
+    return B < (1u << 31) && A < (1u << 31) && F <= 65535 && T < (1u << 31) && ceil_div(B, 4) <= 65535;
+}
+
+}  // namespace
+}  // namespace bb
+
+extern "C" int blade_beamform_f32(const void* in, const void* phasors, void* out, uint64_t B, uint64_t A, uint64_t F,
+                                  uint64_t T, uint64_t P, int incoherent, int incoherent_sqrt, blade_stream_t stream) {
+    using namespace bb;
+    if (P != 1 && P != 2) return set_error(BLADE_ERROR, "blade_beamform_f32: P must be 1 or 2");
+    if (B == 0 && !incoherent) return BLADE_SUCCESS;
+    if (A == 0 || F == 0 || T == 0) return BLADE_SUCCESS;
+    if (!in || !phasors || !out) return set_error(BLADE_ERROR, "blade_beamform_f32: null buffer");
+    if (!dims_ok(B, A, F, T)) return set_error(BLADE_ERROR, "blade_beamform_f32: dimensions out of range");
+    if (incoherent && B == 0) return set_error(BLADE_ERROR, "blade_beamform_f32: incoherent beam needs beam 0");
+    if (P == 2 && (!aligned16(in) || !aligned16(out)))
+        return set_error(BLADE_ERROR, "blade_beamform_f32: dual-pol buffers must be 16-byte aligned");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const float2* ph = static_cast<const float2*>(phasors);
+    const int tg = pick_tg(B);
+    if (P == 2) dispatch_tg<2, IN_CF32, 0>(tg, in, ph, out, B, A, F, T, 1, s);
+    else dispatch_tg<1, IN_CF32, 0>(tg, in, ph, out, B, A, F, T, 1, s);
+    if (incoherent) {
+        if (P == 2)
+            incoherent_kernel<2><<<grid_for(F * T, 256), 256, 0, s>>>(static_cast<const float2*>(in), ph,
+                                                                     static_cast<float2*>(out), (uint32_t)B,
+                                                                     (uint32_t)A, (uint32_t)F, (uint32_t)T,
+                                                                     incoherent_sqrt);
+        else
+            incoherent_kernel<1><<<grid_for(F * T, 256), 256, 0, s>>>(static_cast<const float2*>(in), ph,
+                                                                     static_cast<float2*>(out), (uint32_t)B,
+                                                                     (uint32_t)A, (uint32_t)F, (uint32_t)T,
+                                                                     incoherent_sqrt);
+    }
+    return check_launch("blade_beamform_f32");
+}
+
+extern "C" int blade_beamform_detect_f32(int in_type, const void* in, const void* phasors, void* out, uint64_t B,
+                                         uint64_t A, uint64_t F, uint64_t T, uint64_t P, uint64_t rate,
+                                         uint64_t integration, blade_stream_t stream) {
+    using namespace bb;
+    if (P != 2) return set_error(BLADE_ERROR, "blade_beamform_detect_f32: P must be 2 (Stokes-I detector)");
+    if (rate != 1 && rate != 2 && rate != 4)
+        return set_error(BLADE_ERROR, "blade_beamform_detect_f32: rate must be 1, 2 or 4");
+    if (integration == 0) return set_error(BLADE_ERROR, "blade_beamform_detect_f32: integration must be > 0");
+    if (T % (rate * integration) != 0)
+        return set_error(BLADE_ERROR, "blade_beamform_detect_f32: T must be a multiple of rate * integration");
+    if (in_type != BLADE_CF32 && in_type != BLADE_CI8)
+        return set_error(BLADE_ERROR, "blade_beamform_detect_f32: input type must be CF32 or CI8");
+    if (B == 0 || A == 0 || F == 0 || T == 0) return BLADE_SUCCESS;
+    if (!in || !phasors || !out) return set_error(BLADE_ERROR, "blade_beamform_detect_f32: null buffer");
+    if (!dims_ok(B, A, F, T)) return set_error(BLADE_ERROR, "blade_beamform_detect_f32: dimensions out of range");
+    const uint64_t ns = 4 / rate;  // spectra per thread
+    int tg = pick_tg(B);
+    // The window (rate * integration samples) must tile the CTA's 4 TG samples and
+    // span at most one warp of threads.
+    while (tg < 256 && (4ull * tg) % (rate * integration) != 0) tg *= 2;
+    if ((4ull * tg) % (rate * integration) != 0)
+        return set_error(BLADE_ERROR, "blade_beamform_detect_f32: rate * integration must divide %d", 4 * tg);
+    if (integration > ns) {
+        const uint64_t g = integration / ns;
+        if (integration % ns != 0 || (g & (g - 1)) != 0 || g > 32)
+            return set_error(BLADE_ERROR, "blade_beamform_detect_f32: integration %llu not supported at rate %llu",
+                             (unsigned long long)integration, (unsigned long long)rate);
+    } else if (ns % integration != 0) {
+        return set_error(BLADE_ERROR, "blade_beamform_detect_f32: integration must divide %llu",
+                         (unsigned long long)ns);
+    }
+    if (in_type == BLADE_CF32 && !aligned16(in))
+        return set_error(BLADE_ERROR, "blade_beamform_detect_f32: CF32 input must be 16-byte aligned");
+    if (in_type == BLADE_CI8 && (reinterpret_cast<uintptr_t>(in) & 3))
+        return set_error(BLADE_ERROR, "blade_beamform_detect_f32: CI8 input must be 4-byte aligned");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const float2* ph = static_cast<const float2*>(phasors);
+    if (in_type == BLADE_CI8) {
+        if (rate == 1) dispatch_tg<2, IN_CI8, 1>(tg, in, ph, out, B, A, F, T, integration, s);
+        else if (rate == 2) dispatch_tg<2, IN_CI8, 2>(tg, in, ph, out, B, A, F, T, integration, s);
+        else dispatch_tg<2, IN_CI8, 4>(tg, in, ph, out, B, A, F, T, integration, s);
+    } else {
+        if (rate == 1) dispatch_tg<2, IN_CF32, 1>(tg, in, ph, out, B, A, F, T, integration, s);
+        else if (rate == 2) dispatch_tg<2, IN_CF32, 2>(tg, in, ph, out, B, A, F, T, integration, s);
+        else dispatch_tg<2, IN_CF32, 4>(tg, in, ph, out, B, A, F, T, integration, s);
+    }
+    return check_launch("blade_beamform_detect_f32");
+}

@@ -1,0 +1,727 @@
+"""Modules of the beamform -> channelize -> detect path.
+
+Each class mirrors the reference module of the same name: the ``Config`` fields
+and keyword names of the nanobind bindings (``python/blade/ext_*.cc``), the
+``Input`` fields, the output shape, the taint and compute ratio, and the
+constructor checks (a failed check raises ``RuntimeError``, which is what the
+reference's ``BL_CHECK_THROW`` becomes in Python, ``python/blade/ext_hidden.cc:17-24``).
+``process(step, stream)`` enqueues the module's kernel through the C ABI
+(``libblade_b200.so``) on ``stream`` and returns a ``result`` code.
+
+Output buffers are allocated per Runner slot when the module lives in a
+pipeline (``Duet``), so the two in-flight slots never share an intermediate
+buffer (the reference shares them, ``src/runner.cc:17-68``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from .constants import Taint, pol, result
+from .memory import Duet, Vector, as_vector, element_bytes, type_code
+
+_COMPLEX = {"ci8", "cf16", "cf32", "cf64"}
+
+
+def _stream_handle(stream) -> Optional[int]:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream if torch.cuda.is_available() else None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _fail(msg: str):
+    raise RuntimeError(msg)
+
+
+class Module:
+    """Base class (include/blade/module.hh:20-115)."""
+
+    taint = Taint.NONE
+
+    def __init__(self):
+        self._owned: list = []  # Duets owned by this module (per-slot outputs)
+
+    def get_taint(self) -> Taint:
+        return self.taint
+
+    def get_compute_ratio(self) -> int:
+        return 1
+
+    def name(self) -> str:
+        return type(self).__name__
+
+    def process(self, step: int = 0, stream=None) -> result:  # pragma: no cover - overridden
+        return result.success
+
+    # -- helpers ---------------------------------------------------------------
+    def _alloc(self, shape, dtype, kind="array_tensor"):
+        """Output buffer: one per Runner slot inside a pipeline, else a single Vector."""
+        from .runtime import _fetch_pipeline
+
+        if _fetch_pipeline() is not None:
+            d = Duet(shape, dtype, "cuda", kind)
+            self._owned.append(d)
+            return d
+        return Vector(shape, dtype, "cuda", kind)
+
+    def _set_slot(self, index: int) -> None:
+        for d in self._owned:
+            d.set(index)
+
+    def __repr__(self):
+        return f"{self.name()}()"
+
+
+def _out(buf):
+    return as_vector(buf)
+
+
+# =============================================================================
+# Cast
+# =============================================================================
+
+class Cast(Module):
+    """Modules::Cast<IT, OT> (include/blade/modules/cast.hh, src/modules/cast/base.cc:12-66)."""
+
+    taint = Taint.CONSUMER | Taint.PRODUCER
+
+    @dataclass
+    class config:
+        block_size: int = 512
+
+    @dataclass
+    class input:
+        buffer: object
+
+    def __init__(self, config, input, stream=None, it="cf32", ot="cf32"):
+        super().__init__()
+        self.config, self._input, self._it, self._ot = config, input, it, ot
+        buf = as_vector(input.buffer)
+        if (it in _COMPLEX) != (ot in _COMPLEX):
+            _fail("Cannot cast between complex and non-complex types.")
+        if buf.dtype != it:
+            _fail(f"Cast input buffer is {buf.dtype}, expected {it}.")
+        if it == ot:
+            self._output = input.buffer  # bypass (Link), base.cc:45-49
+        else:
+            self._output = self._alloc(buf.shape, ot)
+
+    def get_config(self):
+        return self.config
+
+    def get_input(self):
+        return self._input.buffer
+
+    def get_output(self):
+        return self._output
+
+    def process(self, step=0, stream=None):
+        if self._it == self._ot:
+            return result.success
+        i, o = as_vector(self._input.buffer), _out(self._output)
+        _lib.call("blade_cast", type_code(self._it), type_code(self._ot), i.data_ptr(), o.data_ptr(), i.size(),
+                  _stream_handle(stream))
+        return result.success
+
+
+# =============================================================================
+# Beamformer (ATA)
+# =============================================================================
+
+class BeamformerATA(Module):
+    """Modules::Beamformer::ATA<CF32, CF32> (include/blade/modules/beamformer/{generic,ata}.hh,
+    src/modules/beamformer/ata.cc:7-74, generic.cc:9-33).
+
+    ``block_size`` is accepted for interface parity; the kernel has no block-size
+    constraint, so the reference's T % blockSize and B <= blockSize checks
+    (generic.cc:17-21, ata.cc:13-17), which only guard its launch geometry, are
+    not applied."""
+
+    taint = Taint.CONSUMER | Taint.PRODUCER
+
+    @dataclass
+    class config:
+        enable_incoherent_beam: bool = False
+        enable_incoherent_beam_sqrt: bool = False
+        block_size: int = 512
+
+    @dataclass
+    class input:
+        buffer: object
+        phasors: object
+
+    def __init__(self, config, input, stream=None, it="cf32", ot="cf32"):
+        super().__init__()
+        self.config, self._input = config, input
+        buf, ph = as_vector(input.buffer), as_vector(input.phasors)
+        if it != "cf32" or ot != "cf32" or buf.dtype != "cf32" or ph.dtype != "cf32":
+            _fail("Beamformer::ATA supports CF32 -> CF32 only.")
+        A, F, T, P = buf.shape
+        B, Ap, Fp, Tp, Pp = ph.shape
+        if Fp != F:
+            _fail(f"Number of frequency channels mismatch between phasors ({Fp}) and buffer ({F}).")
+        if Pp != P:
+            _fail(f"Number of polarizations mismatch between phasors ({Pp}) and buffer ({P}).")
+        if Ap != A:
+            _fail(f"Number of antennas mismatch between phasors ({Ap}) and buffer ({A}).")
+        if Tp != 1:
+            _fail("Phasor time axis must be 1.")
+        self._shape = (B + (1 if config.enable_incoherent_beam else 0), F, T, P)
+        self._output = self._alloc(self._shape, "cf32")
+
+    def get_config(self):
+        return self.config
+
+    def get_input_buffer(self):
+        return self._input.buffer
+
+    def get_input_phasors(self):
+        return self._input.phasors
+
+    def get_output(self):
+        return self._output
+
+    def process(self, step=0, stream=None):
+        buf, ph, out = as_vector(self._input.buffer), as_vector(self._input.phasors), _out(self._output)
+        A, F, T, P = buf.shape
+        B = ph.shape[0]
+        _lib.call("blade_beamform_f32", buf.data_ptr(), ph.data_ptr(), out.data_ptr(), B, A, F, T, P,
+                  int(self.config.enable_incoherent_beam), int(self.config.enable_incoherent_beam_sqrt),
+                  _stream_handle(stream))
+        return result.success
+
+
+# =============================================================================
+# Channelizer
+# =============================================================================
+
+class Channelizer(Module):
+    """Modules::Channelizer<CF32, CF32> (include/blade/modules/channelizer/base.hh:12-87,
+    src/modules/channelizer/base.cc:9-146).
+
+    rate == 1 and rate == T run in place (the reference's Link), any other even
+    rate dividing T (rejected by the reference, base.cc:30-35) writes its own
+    [A, F*rate, T/rate, P] buffer."""
+
+    taint = Taint.CONSUMER | Taint.MODIFIER
+
+    @dataclass
+    class config:
+        rate: int = 4
+        block_size: int = 512
+
+    @dataclass
+    class input:
+        buffer: object
+
+    def __init__(self, config, input, stream=None, it="cf32", ot="cf32"):
+        super().__init__()
+        self.config, self._input = config, input
+        buf = as_vector(input.buffer)
+        if buf.dtype != "cf32":
+            _fail("Channelizer supports CF32 only.")
+        A, F, T, P = buf.shape
+        C = int(config.rate)
+        if C <= 0 or T % C != 0:
+            _fail(f"The number of time samples ({T}) should be divisable by the channelizer rate ({C}).")
+        if C % 2 != 0 and C != 1:
+            _fail(f"The channelizer rate ({C}) should be divisable by 2.")
+        if P not in (1, 2):
+            _fail(f"Number of polarizations ({P}) of the input should be one or two.")
+        self._shape = (A, F * C, T // C, P)
+        self._inplace = C in (1, T)
+        if self._inplace:
+            self._output = _reshaped(input.buffer, self._shape)
+        else:
+            self._output = self._alloc(self._shape, "cf32")
+        wsb = _lib.load().blade_channelize_workspace_size(A, F, T, P, C)
+        self._ws = torch.empty(int(wsb), dtype=torch.uint8, device="cuda") if wsb else None
+
+    def get_config(self):
+        return self.config
+
+    def get_input(self):
+        return self._input.buffer
+
+    def get_output(self):
+        return self._output
+
+    def process(self, step=0, stream=None):
+        if self.config.rate == 1:
+            return result.success
+        buf, out = as_vector(self._input.buffer), _out(self._output)
+        A, F, T, P = buf.shape
+        _lib.call("blade_channelize", buf.data_ptr(), out.data_ptr(),
+                  self._ws.data_ptr() if self._ws is not None else None, A, F, T, P, int(self.config.rate),
+                  _stream_handle(stream))
+        return result.success
+
+
+def _reshaped(buf, shape):
+    v = as_vector(buf)
+    if tuple(v.shape) == tuple(shape):
+        return buf
+    return _ReshapedVector(buf, shape)
+
+
+class _ReshapedVector(Vector):
+    def __init__(self, src, shape):
+        self._src = src
+        v = as_vector(src)
+        self._shape_fixed = shape
+        super().__init__(shape, v.dtype, v.device, "array_tensor", storage=v.as_torch())
+
+    def data_ptr(self):
+        return as_vector(self._src).data_ptr()
+
+    def as_torch(self):
+        return as_vector(self._src).as_torch().reshape(self._shape_fixed if self.dtype not in ("ci8", "cf16")
+                                                       else tuple(self._shape_fixed) + (2,))
+
+
+# =============================================================================
+# Polarizer
+# =============================================================================
+
+class Polarizer(Module):
+    """Modules::Polarizer<T, T> (include/blade/modules/polarizer.hh:9-71,
+    src/modules/polarizer/base.cc:12-68); in place, bypassed when the input and
+    output bases are equal."""
+
+    taint = Taint.MODIFIER
+
+    @dataclass
+    class config:
+        inputPolarization: int = pol.xy
+        outputPolarization: int = pol.lr
+        block_size: int = 512
+
+    @dataclass
+    class input:
+        buffer: object
+
+    def __init__(self, config, input, stream=None, it="cf32", ot="cf32"):
+        super().__init__()
+        self.config, self._input = config, input
+        if it != ot:
+            _fail(f"This module requires the type of the input ({it}) and output ({ot}) to be the same.")
+        buf = as_vector(input.buffer)
+        if buf.dtype not in ("cf32", "cf16"):
+            _fail("Polarizer supports CF32 and CF16.")
+        if buf.shape[3] != 2:
+            _fail("Polarizer needs two polarizations.")
+        self._output = input.buffer
+
+    def get_config(self):
+        return self.config
+
+    def get_input(self):
+        return self._input.buffer
+
+    def get_output(self):
+        return self._output
+
+    def process(self, step=0, stream=None):
+        if int(self.config.inputPolarization) == int(self.config.outputPolarization):
+            return result.success
+        buf = as_vector(self._input.buffer)
+        A, F, T, P = buf.shape
+        _lib.call("blade_polarize", type_code(buf.dtype), buf.data_ptr(), buf.data_ptr(), A * F * T,
+                  _stream_handle(stream))
+        return result.success
+
+
+# =============================================================================
+# Detector
+# =============================================================================
+
+class Detector(Module):
+    """Modules::Detector<CF32, F32> (include/blade/modules/detector.hh:12-81,
+    src/modules/detector/base.cc:9-85)."""
+
+    taint = Taint.CONSUMER | Taint.PRODUCER
+
+    @dataclass
+    class config:
+        integration_size: int = 1
+        number_of_output_polarizations: int = 4
+        block_size: int = 512
+
+    @dataclass
+    class input:
+        buffer: object
+
+    def __init__(self, config, input, stream=None, it="cf32", ot="f32"):
+        super().__init__()
+        self.config, self._input = config, input
+        buf = as_vector(input.buffer)
+        if buf.dtype != "cf32" or ot != "f32":
+            _fail("Detector supports CF32 -> F32 only.")
+        A, F, T, P = buf.shape
+        I = int(config.integration_size)
+        if I <= 0:
+            _fail(f"Integration size ({I}) should be more than zero.")
+        if T % I != 0:
+            _fail(f"The number of time samples ({T}) should be divisable by the integration size ({I}).")
+        if P != 2:
+            _fail(f"Number of polarizations ({P}) should be two (2).")
+        if A <= 0:
+            _fail(f"Number of aspects ({A}) should be more than zero.")
+        if config.number_of_output_polarizations not in (1, 4):
+            _fail(f"Number of output polarizations ({config.number_of_output_polarizations}) not supported.")
+        self._shape = (A, F, T // I, int(config.number_of_output_polarizations))
+        self._output = self._alloc(self._shape, "f32")
+
+    def get_config(self):
+        return self.config
+
+    def get_input(self):
+        return self._input.buffer
+
+    def get_output(self):
+        return self._output
+
+    def process(self, step=0, stream=None):
+        buf, out = as_vector(self._input.buffer), _out(self._output)
+        A, F, T, P = buf.shape
+        _lib.call("blade_detect", buf.data_ptr(), out.data_ptr(), A, F, T, P, int(self.config.integration_size),
+                  int(self.config.number_of_output_polarizations), _stream_handle(stream))
+        return result.success
+
+
+# =============================================================================
+# Gather
+# =============================================================================
+
+class Gather(Module):
+    """Modules::Gather<T, T> (include/blade/modules/gather.hh:12-95,
+    src/modules/gather/base.cc:12-111); CHRONOUS with compute ratio = multiplier."""
+
+    taint = Taint.CONSUMER | Taint.PRODUCER | Taint.CHRONOUS
+
+    @dataclass
+    class config:
+        axis: int = 0
+        multiplier: int = 1
+        copy_size_threshold: int = 512
+        block_size: int = 512
+
+    @dataclass
+    class input:
+        buffer: object
+
+    def __init__(self, config, input, stream=None, it="cf32", ot="cf32"):
+        super().__init__()
+        self.config, self._input = config, input
+        if it != ot:
+            _fail(f"Input ({it}) and output ({ot}) types aren't the same. Casting isn't supported by Gather yet.")
+        buf = as_vector(input.buffer)
+        if config.axis >= 4:
+            _fail(f"Selected input axis ({config.axis}) is larger than input shape dimensions (4).")
+        if config.multiplier <= 0:
+            _fail(f"Multiplier ({config.multiplier}) should be more than zero.")
+        shape = list(buf.shape)
+        shape[config.axis] *= config.multiplier
+        self._shape = tuple(shape)
+        self._output = self._alloc(self._shape, buf.dtype)
+
+    def get_compute_ratio(self):
+        return int(self.config.multiplier)
+
+    def get_config(self):
+        return self.config
+
+    def get_input(self):
+        return self._input.buffer
+
+    def get_output(self):
+        return self._output
+
+    def process(self, step=0, stream=None):
+        buf, out = as_vector(self._input.buffer), _out(self._output)
+        shape = _lib.u64_array(buf.shape)
+        _lib.call("blade_gather", element_bytes(buf.dtype), buf.data_ptr(), out.data_ptr(), shape,
+                  int(self.config.axis), int(self.config.multiplier), int(step), _stream_handle(stream))
+        return result.success
+
+
+# =============================================================================
+# Permutation
+# =============================================================================
+
+class Permutation(Module):
+    """Modules::Permutation<T, T> (include/blade/modules/permutation.hh:11-78,
+    src/modules/permutation/base.cc:12-73)."""
+
+    taint = Taint.CONSUMER | Taint.PRODUCER
+
+    @dataclass
+    class config:
+        indexes: Sequence[int] = (0, 1, 2, 3)
+        block_size: int = 512
+
+    @dataclass
+    class input:
+        buffer: object
+
+    def __init__(self, config, input, stream=None, it="cf32", ot="cf32"):
+        super().__init__()
+        self.config, self._input = config, input
+        if it != ot:
+            _fail(f"Input ({it}) and output ({ot}) types aren't the same. "
+                  "Casting isn't supported by Permutation yet.")
+        buf = as_vector(input.buffer)
+        idx = [int(i) for i in config.indexes]
+        if len(idx) != 4:
+            _fail(f"Selected input rank ({len(idx)}) doesn't match input shape rank (4).")
+        if len(set(idx)) != 4:
+            dup = [i for i in idx if idx.count(i) > 1][0]
+            _fail(f"Repeated index {dup} in permutation.")
+        if any(i < 0 or i > 3 for i in idx):
+            _fail("Permutation index out of range.")
+        self._idx = idx
+        self._shape = tuple(buf.shape[i] for i in idx)
+        self._output = self._alloc(self._shape, buf.dtype)
+
+    def get_config(self):
+        return self.config
+
+    def get_input(self):
+        return self._input.buffer
+
+    def get_output(self):
+        return self._output
+
+    def process(self, step=0, stream=None):
+        buf, out = as_vector(self._input.buffer), _out(self._output)
+        _lib.call("blade_permute", element_bytes(buf.dtype), buf.data_ptr(), out.data_ptr(),
+                  _lib.u64_array(buf.shape), _lib.u64_array(self._idx), _stream_handle(stream))
+        return result.success
+
+
+# =============================================================================
+# Duplicate
+# =============================================================================
+
+class Duplicate(Module):
+    """Modules::Duplicate<T, T> (include/blade/modules/duplicate.hh:11-64,
+    src/modules/duplicate/base.cc:12-37)."""
+
+    taint = Taint.CONSUMER | Taint.PRODUCER
+
+    @dataclass
+    class config:
+        pass
+
+    @dataclass
+    class input:
+        buffer: object
+
+    def __init__(self, config, input, stream=None, it="cf32", ot="cf32"):
+        super().__init__()
+        self.config, self._input = config, input
+        if it != ot:
+            _fail(f"Input ({it}) and output ({ot}) types aren't the same. "
+                  "Casting isn't supported by Duplicate yet.")
+        buf = as_vector(input.buffer)
+        self._output = self._alloc(buf.shape, buf.dtype)
+
+    def get_config(self):
+        return self.config
+
+    def get_input(self):
+        return self._input.buffer
+
+    def get_output(self):
+        return self._output
+
+    def process(self, step=0, stream=None):
+        buf, out = as_vector(self._input.buffer), _out(self._output)
+        _lib.call("blade_duplicate", buf.data_ptr(), out.data_ptr(), buf.nbytes, _stream_handle(stream))
+        return result.success
+
+
+# =============================================================================
+# Phasor (delay -> phasor)
+# =============================================================================
+
+class Phasor(Module):
+    """Delay -> phasor part of Modules::Phasor::ATA<CF32> (src/modules/phasor/ata.cc:176-208),
+    on the GPU in FP64.  The geometric-delay half of the reference module (ERFA
+    astrometry, ata.cc:9-173) is replaced by a delays input: [B, A] seconds."""
+
+    taint = Taint.CONSUMER | Taint.PRODUCER
+
+    @dataclass
+    class config:
+        number_of_beams: int = 1
+        number_of_antennas: int = 1
+        number_of_frequency_channels: int = 1
+        number_of_polarizations: int = 2
+        observation_frequency_hz: float = 0.0
+        channel_bandwidth_hz: float = 0.0
+        total_bandwidth_hz: float = 0.0
+        frequency_start_index: int = 0
+        antenna_calibrations: object = None  # CF64 [A, F, 1, P] (numpy or Vector), None = unit
+        block_size: int = 512
+
+    @dataclass
+    class input:
+        delays: object  # F64 delay_tensor [B, A] on the device
+
+    def __init__(self, config, input, stream=None, it="f64", ot="cf32"):
+        super().__init__()
+        self.config, self._input = config, input
+        c = config
+        d = as_vector(input.delays)
+        if d.dtype != "f64" or tuple(d.shape) != (c.number_of_beams, c.number_of_antennas):
+            _fail("Phasor delays must be an F64 delay_tensor [B, A].")
+        self._cal = None
+        if c.antenna_calibrations is not None:
+            cal = c.antenna_calibrations
+            arr = cal.as_numpy() if isinstance(cal, Vector) else np.asarray(cal)
+            exp = (c.number_of_antennas, c.number_of_frequency_channels, 1, c.number_of_polarizations)
+            if tuple(arr.shape) != exp:
+                _fail(f"Calibrations shape {arr.shape} != {exp}.")
+            self._cal = torch.from_numpy(np.ascontiguousarray(arr, dtype=np.complex128)).cuda()
+        self._shape = (c.number_of_beams, c.number_of_antennas, c.number_of_frequency_channels, 1,
+                       c.number_of_polarizations)
+        self._output = self._alloc(self._shape, "cf32", "phasor_tensor")
+
+    def get_config(self):
+        return self.config
+
+    def get_phasors(self):
+        return self._output
+
+    get_output = get_phasors
+
+    def process(self, step=0, stream=None):
+        c = self.config
+        d, out = as_vector(self._input.delays), _out(self._output)
+        _lib.call("blade_phasor_from_delays", d.data_ptr(), self._cal.data_ptr() if self._cal is not None else None,
+                  out.data_ptr(), c.number_of_beams, c.number_of_antennas, c.number_of_frequency_channels,
+                  c.number_of_polarizations, float(c.observation_frequency_hz), float(c.channel_bandwidth_hz),
+                  float(c.total_bandwidth_hz), int(c.frequency_start_index), _stream_handle(stream))
+        return result.success
+
+
+# =============================================================================
+# Fused chain: Cast -> Beamformer -> Channelizer -> Detector (Stokes-I)
+# =============================================================================
+
+class BeamformDetect(Module):
+    """The beamform + channelize + detect chain of Bundles::ATA::ModeB
+    (include/blade/bundles/ata/mode_b.hh:99-199: Beamformer -> [Channelizer] ->
+    Detector) as one fused launch.
+
+    precision = "fp16_split": tcgen05 tensor cores, CI8 input, FP16 hi+lo phasors,
+    FP32 accumulation in TMEM.  precision = "fp32": FP32 CUDA cores (CI8 or CF32
+    input).  "auto" takes the tensor-core path whenever the shape allows it."""
+
+    taint = Taint.CONSUMER | Taint.PRODUCER
+
+    @dataclass
+    class config:
+        rate: int = 1
+        integration_size: int = 1
+        number_of_output_polarizations: int = 1
+        precision: str = "auto"
+        block_size: int = 512
+
+    @dataclass
+    class input:
+        buffer: object
+        phasors: object
+
+    def __init__(self, config, input, stream=None, it="ci8", ot="f32"):
+        super().__init__()
+        self.config, self._input = config, input
+        buf, ph = as_vector(input.buffer), as_vector(input.phasors)
+        if buf.dtype not in ("ci8", "cf32") or ph.dtype != "cf32" or ot != "f32":
+            _fail("BeamformDetect takes CI8 or CF32 voltages, CF32 phasors and produces F32.")
+        if config.number_of_output_polarizations != 1:
+            _fail("BeamformDetect produces Stokes-I (number_of_output_polarizations = 1).")
+        A, F, T, P = buf.shape
+        B = ph.shape[0]
+        if tuple(ph.shape) != (B, A, F, 1, P):
+            _fail(f"Phasor shape {tuple(ph.shape)} does not match voltages {tuple(buf.shape)}.")
+        R, I = int(config.rate), int(config.integration_size)
+        if R <= 0 or I <= 0 or T % (R * I) != 0:
+            _fail(f"T ({T}) must be a multiple of rate ({R}) x integration ({I}).")
+        lib = _lib.load()
+        tc_ok = buf.dtype == "ci8" and lib.blade_beamform_detect_tc_supported(B, A, F, T, P, R, I) == 1
+        prec = config.precision
+        if prec == "auto":
+            prec = "fp16_split" if tc_ok else "fp32"
+        if prec == "fp16_split" and not tc_ok:
+            _fail("The tensor-core path needs CI8 input, P = 2, A <= 64, T % 128 == 0, rate in {1, 2, 4} and an "
+                  "integration that is a power of two <= 32.")
+        if prec not in ("fp16_split", "fp32"):
+            _fail(f"Unknown precision {prec!r}.")
+        self.precision = prec
+        self._shape = (B, F * R, T // (R * I), 1)
+        self._output = self._alloc(self._shape, "f32")
+        self._plan = None
+        if prec == "fp16_split":
+            n = int(lib.blade_beamform_tc_plan_size(B, A, F, P))
+            self._plan = torch.empty(n, dtype=torch.uint8, device="cuda")
+
+    def get_config(self):
+        return self.config
+
+    def get_input_buffer(self):
+        return self._input.buffer
+
+    def get_input_phasors(self):
+        return self._input.phasors
+
+    def get_output(self):
+        return self._output
+
+    def process(self, step=0, stream=None):
+        buf, ph, out = as_vector(self._input.buffer), as_vector(self._input.phasors), _out(self._output)
+        A, F, T, P = buf.shape
+        B = ph.shape[0]
+        R, I = int(self.config.rate), int(self.config.integration_size)
+        s = _stream_handle(stream)
+        if self.precision == "fp16_split":
+            _lib.call("blade_beamform_tc_prepare", ph.data_ptr(), self._plan.data_ptr(), B, A, F, P, s)
+            _lib.call("blade_beamform_detect_tc", buf.data_ptr(), self._plan.data_ptr(), out.data_ptr(), B, A, F, T,
+                      P, R, I, s)
+        else:
+            _lib.call("blade_beamform_detect_f32", type_code(buf.dtype), buf.data_ptr(), ph.data_ptr(),
+                      out.data_ptr(), B, A, F, T, P, R, I, s)
+        return result.success
+
+
+# Registry used by blade_b200.module(): (name, telescope) -> (class, {(it, ot)}).
+_CAST_PAIRS = {("i8", "i8"), ("i8", "f32"), ("f16", "f32"), ("f16", "f16"), ("f32", "i32"), ("f32", "f16"),
+               ("f32", "f32"), ("ci8", "cf32"), ("ci8", "cf16"), ("ci8", "ci8"), ("cf32", "cf16"),
+               ("cf32", "cf32"), ("cf16", "cf32"), ("cf16", "cf16"),
+               # instantiated by the reference but rejected at construction (complex <-> real)
+               ("f16", "cf32"), ("f16", "cf16"), ("f32", "cf32"), ("f32", "cf16"), ("cf32", "f16"),
+               ("cf32", "f32"), ("cf16", "f16"), ("cf16", "f32")}
+
+REGISTRY = {
+    ("cast", "generic"): (Cast, _CAST_PAIRS),
+    ("beamformer", "ata"): (BeamformerATA, {("cf32", "cf32")}),
+    ("channelizer", "generic"): (Channelizer, {("cf32", "cf32")}),
+    ("polarizer", "generic"): (Polarizer, {("cf32", "cf32"), ("cf16", "cf16")}),
+    ("detector", "generic"): (Detector, {("cf32", "f32")}),
+    ("gather", "generic"): (Gather, {("f32", "f32"), ("cf32", "cf32"), ("cf16", "cf16"), ("ci8", "ci8")}),
+    ("permutation", "generic"): (Permutation, {("cf32", "cf32"), ("cf16", "cf16"), ("ci8", "ci8")}),
+    ("duplicate", "generic"): (Duplicate, {("cf32", "cf32"), ("cf16", "cf16"), ("ci8", "ci8"), ("f32", "f32")}),
+    ("phasor", "ata"): (Phasor, {("f64", "cf32")}),
+    ("phasor", "generic"): (Phasor, {("f64", "cf32")}),
+    ("beamform_detect", "ata"): (BeamformDetect, {("ci8", "f32"), ("cf32", "f32")}),
+    ("beamform_detect", "generic"): (BeamformDetect, {("ci8", "f32"), ("cf32", "f32")}),
+}

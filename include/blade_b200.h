@@ -1,0 +1,230 @@
+/*
+ * blade_b200 C ABI: the drop-in boundary of the B200-native beamform ->
+ * channelize -> detect path.
+ *
+ * Every entry point takes raw device pointers, shape integers, configuration
+ * scalars and a CUDA stream (a cudaStream_t; NULL is the legacy default stream),
+ * enqueues its work asynchronously on that stream, and returns a status code
+ * that mirrors Blade::Result (reference include/blade/macros.hh:31-48):
+ * 0 = SUCCESS, 1 = ERROR (bad shape or configuration, nothing enqueued),
+ * 2 = CUDA_ERROR (a launch failed), 3 = ASSERTION_ERROR.  The message of the
+ * last failure on the calling thread is returned by blade_last_error().
+ *
+ * Layouts are the reference's, row-major with the last axis innermost:
+ *   ArrayShape  [A, F, T, P]     (include/blade/memory/custom.hh:10-53)
+ *   PhasorShape [B, A, F, 1, P]  (include/blade/memory/custom.hh:55-103)
+ *   DelayShape  [B, A]           (include/blade/memory/custom.hh:105-138)
+ * Complex values are interleaved (re, im) pairs of the scalar type.
+ */
+#ifndef BLADE_B200_H
+#define BLADE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* blade_stream_t; /* same type as cudaStream_t */
+
+#if defined(__GNUC__)
+#define BLADE_API __attribute__((visibility("default")))
+#else
+#define BLADE_API
+#endif
+
+/* Status codes (Blade::Result, include/blade/macros.hh:31-48). */
+#define BLADE_SUCCESS 0
+#define BLADE_ERROR 1
+#define BLADE_CUDA_ERROR 2
+#define BLADE_ASSERTION_ERROR 3
+
+/* Element types (the reference's I8, I32, F16, F32, F64, CI8, CF16, CF32, CF64;
+ * include/blade/memory/types.hh). */
+#define BLADE_I8 1
+#define BLADE_I32 2
+#define BLADE_F16 3
+#define BLADE_F32 4
+#define BLADE_F64 5
+#define BLADE_CI8 6
+#define BLADE_CF16 7
+#define BLADE_CF32 8
+#define BLADE_CF64 9
+
+/* Message of the last failure on this thread ("" if none). */
+BLADE_API const char* blade_last_error(void);
+
+/* ABI version: major * 10000 + minor * 100 + patch. */
+BLADE_API int blade_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Cast: out[i] = static_cast<OT>(in[i]) over the scalar subtype; n_elements
+ * counts elements of the input type (a complex element is two scalars).
+ * Complex <-> real casts are rejected with BLADE_ERROR.  Bit-exact.
+ * Replaces Modules::Cast<IT,OT>::process, src/modules/cast/base.cc:60-66 and
+ * the kernel src/modules/cast/cast.cu:5-12.
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_cast(int in_type, int out_type, const void* in, void* out,
+               uint64_t n_elements, blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Phasors from delays, in FP64 with FP64 argument reduction:
+ *   phasors[b,a,f,0,p] = exp(-i 2 pi tau[b,a] ((f + freq_start_index) * chan_bw_hz))
+ *                      * exp(-i 2 pi tau[b,a] (obs_freq_hz - total_bw_hz / 2))
+ *                      * calibrations[a,f,0,p]
+ * delays: F64 [B,A] (seconds); calibrations: CF64 [A,F,1,P] or NULL (unit);
+ * phasors: CF32 [B,A,F,1,P].
+ * Replaces the formula half of Modules::Phasor::ATA<CF32>::process,
+ * src/modules/phasor/ata.cc:176-208 (host FP64 loops there).
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_phasor_from_delays(const double* delays, const void* calibrations,
+                             void* phasors, uint64_t B, uint64_t A, uint64_t F,
+                             uint64_t P, double obs_freq_hz, double chan_bw_hz,
+                             double total_bw_hz, uint64_t freq_start_index,
+                             blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Plain FP32 CUDA-core beamformer (the drop-in):
+ *   out[b,f,t,p] = sum_a in[a,f,t,p] * phasors[b,a,f,0,p]   (no conjugate)
+ * in: CF32 [A,F,T,P]; phasors: CF32 [B,A,F,1,P]; out: CF32 [B+inc,F,T,P].
+ * incoherent != 0 adds beam B = (sum_a |in * phasors[0]|^2 [sqrt], 0).
+ * Any A, B, F, T; P in {1, 2}.
+ * Replaces Modules::Beamformer::ATA<CF32,CF32> (src/modules/beamformer/ata.cc:7-74,
+ * generic.cc:30-33) and its kernel src/modules/beamformer/beamformer.cu:13-79.
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_beamform_f32(const void* in, const void* phasors, void* out,
+                       uint64_t B, uint64_t A, uint64_t F, uint64_t T, uint64_t P,
+                       int incoherent, int incoherent_sqrt, blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Channelizer: [A,F,T,P] CF32 -> [A,F*rate,T/rate,P] CF32,
+ *   out[a, f*rate + k, s, p] = fftshift(FFT_rate(in[a, f, s*rate:(s+1)*rate, p]))[k]
+ * unnormalised, hand-written FP32 Stockham FFT.  rate = 1 copies (or is a no-op
+ * when in == out); rate must be even, T % rate == 0, P in {1, 2}, and every
+ * prime factor of rate at most 61.  When rate == T the transform may run in
+ * place (in == out).  Rates above 4096 need a workspace of
+ * blade_channelize_workspace_size() bytes (NULL otherwise).
+ * Replaces Modules::Channelizer<CF32,CF32>::process, src/modules/channelizer/
+ * base.cc:122-146 (pre_channelizer kernel channelizer.cu:5-19 + cuFFT), and
+ * lifts its rate == T restriction (base.cc:30-35).
+ * ------------------------------------------------------------------------- */
+BLADE_API uint64_t blade_channelize_workspace_size(uint64_t A, uint64_t F, uint64_t T,
+                                         uint64_t P, uint64_t rate);
+BLADE_API int blade_channelize(const void* in, void* out, void* workspace,
+                     uint64_t A, uint64_t F, uint64_t T, uint64_t P, uint64_t rate,
+                     blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Polarizer: per dual-pol sample (X, Y) -> (X + iY, X - iY); in may equal out.
+ * type in {BLADE_CF32, BLADE_CF16}; n_samples = A*F*T (P must be 2).
+ * Replaces Modules::Polarizer::process, src/modules/polarizer/base.cc:61-68
+ * and src/modules/polarizer/polarizer.cu:5-25.
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_polarize(int type, const void* in, void* out, uint64_t n_samples,
+                   blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Detector: [A,F,T,2] CF32 -> [A,F,T/I,out_pols] F32, deterministic sums.
+ * out_pols = 4: (|X|^2, |Y|^2, Re X conj Y, Im X conj Y); 1: Stokes-I.
+ * Replaces Modules::Detector<CF32,F32>::process, src/modules/detector/base.cc:
+ * 82-85 and src/modules/detector/detector.cu:7-51 (atomicAdd there).
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_detect(const void* in, void* out, uint64_t A, uint64_t F, uint64_t T,
+                 uint64_t P, uint64_t integration, uint64_t out_pols,
+                 blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Gather: copies block `step` of `multiplier` into out along `axis`:
+ *   out.shape = in.shape with shape[axis] *= multiplier,
+ *   out[..., i + step * shape[axis], ...] = in[..., i, ...].  Bit-exact.
+ * Replaces Modules::Gather::process, src/modules/gather/base.cc:70-111
+ * (kernel gather.cu:6-18 or Copy2D).
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_gather(uint64_t elem_bytes, const void* in, void* out,
+                 const uint64_t shape[4], uint64_t axis, uint64_t multiplier,
+                 uint64_t step, blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Permutation: out.shape[i] = in.shape[indexes[i]]; bit-exact element moves.
+ * Replaces Modules::Permutation::process, src/modules/permutation/base.cc:70-73
+ * and src/modules/permutation/permutation.cu:6-20.
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_permute(uint64_t elem_bytes, const void* in, void* out,
+                  const uint64_t shape[4], const uint64_t indexes[4],
+                  blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Duplicate: device-to-device copy of `bytes` bytes.  Bit-exact.
+ * Replaces Modules::Duplicate::process, src/modules/duplicate/base.cc:34-37.
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_duplicate(const void* in, void* out, uint64_t bytes, blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Fused FP32 CUDA-core chain Cast -> Beamformer -> Channelizer(rate) -> Detector
+ * (Stokes-I), in one pass over the voltages:
+ *   out[b, f*rate + k, u, 0] = sum_{s in window u} sum_p |Y[b, f*rate+k, s, p]|^2
+ * in_type in {BLADE_CI8, BLADE_CF32}; phasors CF32 [B,A,F,1,P]; P = 2;
+ * rate in {1, 2, 4}; out F32 [B, F*rate, T/rate/integration, 1].
+ * Composes src/modules/cast/cast.cu, beamformer.cu:13-62, channelizer
+ * (channelizer.cu + cuFFT) and detector.cu:34-51 of the reference.
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_beamform_detect_f32(int in_type, const void* in, const void* phasors,
+                              void* out, uint64_t B, uint64_t A, uint64_t F,
+                              uint64_t T, uint64_t P, uint64_t rate,
+                              uint64_t integration, blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Tensor-core (tcgen05, sm_100a) chain CI8 -> Beamformer -> Channelizer(rate)
+ * -> Detector (Stokes-I).  CI8 voltages enter the MMA exactly as FP16 (rate 2
+ * and 4 DFTs are folded into the operand build, still exact); each CF32 phasor
+ * is split into an FP16 hi + lo pair whose two products accumulate in FP32 in
+ * tensor memory.
+ * blade_beamform_tc_plan_size / _prepare turn phasors CF32 [B,A,F,1,P] into the
+ * split operand image ("plan", device memory of plan_size bytes; 0 = shape not
+ * supported).  blade_beamform_detect_tc runs the chain;
+ * out F32 [B, F*rate, T/rate/I, 1].
+ * Limits (blade_beamform_detect_tc_supported() returns 1 when met): P = 2,
+ * 1 <= A <= 64, any B (64 beams per pass), T % 128 == 0, rate in {1, 2, 4},
+ * I a power of two <= 32.  Input and plan 16-byte aligned.
+ * Composes the same reference stages as blade_beamform_detect_f32.
+ * ------------------------------------------------------------------------- */
+BLADE_API uint64_t blade_beamform_tc_plan_size(uint64_t B, uint64_t A, uint64_t F, uint64_t P);
+BLADE_API int blade_beamform_tc_prepare(const void* phasors, void* plan, uint64_t B,
+                              uint64_t A, uint64_t F, uint64_t P,
+                              blade_stream_t stream);
+BLADE_API int blade_beamform_detect_tc_supported(uint64_t B, uint64_t A, uint64_t F,
+                                       uint64_t T, uint64_t P, uint64_t rate,
+                                       uint64_t integration);
+BLADE_API int blade_beamform_detect_tc(const void* in, const void* plan, void* out,
+                             uint64_t B, uint64_t A, uint64_t F, uint64_t T,
+                             uint64_t P, uint64_t rate, uint64_t integration,
+                             blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Device-side status of the pipelined kernels: every wait inside them is
+ * bounded, and a wait that expires records a non-zero code here instead of
+ * hanging (the kernel then drains its own work and returns).  Synchronous:
+ * reads and clears the word.  The reference's equivalent is the sticky-error
+ * peek after each launch (include/blade/module.hh:77-80).
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_device_status(uint32_t* status);
+
+/* ---------------------------------------------------------------------------
+ * Adjoint of beamform + Stokes-I detect (no reference counterpart).
+ * For L = -sum_{b,f,t,p} |y[b,f,t,p]|^2, y = beamform(in, phasors):
+ *   grad[b,a,f,0,p] = dL/d conj(w) = -sum_t y[b,f,t,p] conj(in[a,f,t,p])
+ * (beam voltages recomputed tile by tile, never stored).  in CF32 [A,F,T,P],
+ * phasors CF32 [B,A,F,1,P], grad CF32 [B,A,F,1,P]; loss (optional, device F64
+ * scalar) receives L.  The gradient with respect to (Re w, Im w) is
+ * (2 Re grad, 2 Im grad).
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_beamform_detect_adjoint(const void* in, const void* phasors, void* grad,
+                                  double* loss, uint64_t B, uint64_t A, uint64_t F,
+                                  uint64_t T, uint64_t P, blade_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BLADE_B200_H */

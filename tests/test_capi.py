@@ -1,0 +1,93 @@
+"""CPU: the C-ABI library loads, exports every entry point include/blade_b200.h
+declares, and its host-side validation returns the reference's error codes
+without touching a GPU."""
+
+import ctypes
+import os
+import re
+
+import pytest
+
+from blade_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "blade_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"BLADE_API\s+[\w\s\*]+?\b(blade_\w+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert len(syms) >= 19
+    for s in ["blade_cast", "blade_beamform_f32", "blade_channelize", "blade_detect", "blade_beamform_detect_tc",
+              "blade_beamform_detect_adjoint", "blade_phasor_from_delays"]:
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    for s in declared_symbols():
+        assert hasattr(lib, s), s
+        assert s in _lib.exported_symbols(), f"{s} has no ctypes signature"
+
+
+def test_version():
+    assert _lib.load().blade_version() == 10000
+
+
+def _err(name, *args):
+    st = getattr(_lib.load(), name)(*args)
+    return st, _lib.last_error()
+
+
+def test_detect_validation():
+    st, msg = _err("blade_detect", None, None, 2, 4, 10, 2, 3, 1, None)
+    assert st == _lib.ERROR and "divisible" in msg
+    st, msg = _err("blade_detect", None, None, 2, 4, 10, 1, 2, 1, None)
+    assert st == _lib.ERROR and "two (2)" in msg
+    st, msg = _err("blade_detect", None, None, 2, 4, 10, 2, 2, 3, None)
+    assert st == _lib.ERROR and "not supported" in msg
+
+
+@pytest.mark.parametrize("T,P,rate", [(1024, 1, 1025), (1025, 1, 1025), (1025, 4, 1025), (100, 2, 7)])
+def test_channelize_rejects_like_reference(T, P, rate):
+    # The reference's should_fail cases (tests/modules/channelizer/meson.build:31-57)
+    # that stay errors here: odd rate, rate not dividing T, P not in {1, 2}.
+    st, msg = _err("blade_channelize", None, None, None, 8, 128, T, P, rate, None)
+    assert st == _lib.ERROR
+
+
+def test_cast_rejects_complex_to_real():
+    st, msg = _err("blade_cast", _lib.CF32, _lib.F32, None, None, 10, None)
+    assert st == _lib.ERROR and "complex" in msg
+
+
+def test_gather_and_permute_validation():
+    shape = _lib.u64_array([2, 3, 4, 5])
+    st, msg = _err("blade_gather", 8, None, None, shape, 4, 2, 0, None)
+    assert st == _lib.ERROR and "axis" in msg
+    st, msg = _err("blade_gather", 8, None, None, shape, 1, 0, 0, None)
+    assert st == _lib.ERROR and "multiplier" in msg
+    st, msg = _err("blade_permute", 8, None, None, shape, _lib.u64_array([0, 1, 1, 3]), None)
+    assert st == _lib.ERROR and "Repeated" in msg or "repeated" in msg
+
+
+def test_tc_support_query():
+    lib = _lib.load()
+    assert lib.blade_beamform_detect_tc_supported(64, 64, 256, 8192, 2, 1, 8) == 1
+    assert lib.blade_beamform_detect_tc_supported(16, 28, 192, 8192, 2, 4, 4) == 1
+    assert lib.blade_beamform_detect_tc_supported(16, 65, 192, 8192, 2, 4, 4) == 0  # A > 64
+    assert lib.blade_beamform_detect_tc_supported(16, 28, 192, 8000, 2, 4, 4) == 0  # T % 128
+    assert lib.blade_beamform_detect_tc_supported(16, 28, 192, 8192, 2, 8, 4) == 0  # rate
+    assert lib.blade_beamform_detect_tc_supported(16, 28, 192, 8192, 2, 4, 3) == 0  # integration
+    assert lib.blade_beamform_tc_plan_size(64, 64, 256, 2) == 256 * 12 * 64 * 64 * 2
+    assert lib.blade_beamform_tc_plan_size(100, 20, 3, 2) == 2 * 3 * 12 * 64 * 32 * 2
+
+
+def test_channelize_workspace_size():
+    lib = _lib.load()
+    assert lib.blade_channelize_workspace_size(1, 64, 1 << 20, 2, 4096) == 0
+    assert lib.blade_channelize_workspace_size(1, 64, 1 << 20, 2, 65536) == 64 * (1 << 20) * 2 * 8

@@ -1,0 +1,123 @@
+"""GPU parity of the fused beamform -> channelize -> detect chains (FP32 CUDA
+cores and FP16-split tcgen05 tensor cores) and of the adjoint, against the FP64
+oracle, on the workload shapes (channel count reduced so the oracle stays fast).
+
+The tensor-core path's Stokes-I error bound is the north star's 1e-5 relative L2
+against FP64; the FP32 path must meet the same bound."""
+
+import numpy as np
+import pytest
+import torch
+
+import blade_b200 as bl
+from blade_b200 import _lib, synthetic as S
+from oracle import formulas as O
+from tests.gpu_util import c64, call, dev, host, ptr, rel_l2, stream
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+# (name, A, F, T, B, rate, integ) -- workloads 1-3 with F reduced for the oracle
+CHAINS = [
+    ("ata-small", 20, 96, 256, 8, 1, 4),
+    ("ata-production", 28, 12, 8192, 16, 4, 4),
+    ("dense-64x64", 64, 6, 8192, 64, 1, 8),
+    ("rate2", 28, 4, 1024, 16, 2, 8),
+    ("ragged-beams", 13, 3, 512, 37, 4, 2),
+    ("many-beams", 9, 2, 256, 100, 1, 1),
+    ("window32", 16, 2, 1024, 16, 1, 32),
+]
+
+
+def make(A, F, T, B, seed):
+    rng = np.random.default_rng(seed)
+    x = S.ci8_voltages(rng, (A, F, T, 2))
+    _, w = S.phasors(rng, B, A, F)
+    return x, w.astype(np.complex64)
+
+
+@pytest.mark.parametrize("name,A,F,T,B,R,I", CHAINS)
+def test_fused_f32_chain(cuda, name, A, F, T, B, R, I):
+    x, w = make(A, F, T, B, 1)
+    ref = O.beamform_channelize_detect(x, w, R, I)
+    xd, wd = dev(x), c64(w)
+    od = torch.zeros((B, F * R, T // (R * I), 1), dtype=torch.float32, device="cuda")
+    call("blade_beamform_detect_f32", _lib.CI8, ptr(xd), ptr(wd), ptr(od), B, A, F, T, 2, R, I, stream())
+    assert rel_l2(host(od), ref) < TOL
+
+
+@pytest.mark.parametrize("name,A,F,T,B,R,I", CHAINS)
+def test_tensor_core_chain(cuda, name, A, F, T, B, R, I):
+    x, w = make(A, F, T, B, 2)
+    ref = O.beamform_channelize_detect(x, w, R, I)
+    lib = _lib.load()
+    assert lib.blade_beamform_detect_tc_supported(B, A, F, T, 2, R, I) == 1
+    xd, wd = dev(x), c64(w)
+    plan = torch.empty(int(lib.blade_beamform_tc_plan_size(B, A, F, 2)), dtype=torch.uint8, device="cuda")
+    od = torch.full((B, F * R, T // (R * I), 1), float("nan"), dtype=torch.float32, device="cuda")
+    call("blade_beamform_tc_prepare", ptr(wd), ptr(plan), B, A, F, 2, stream())
+    call("blade_beamform_detect_tc", ptr(xd), ptr(plan), ptr(od), B, A, F, T, 2, R, I, stream())
+    y = host(od)
+    assert bl.device_status() == 0
+    assert np.isfinite(y).all()
+    err = rel_l2(y, ref)
+    print(f"{name}: Stokes-I relative L2 vs FP64 = {err:.3e}")
+    assert err < TOL
+    # deterministic
+    od2 = torch.zeros_like(od)
+    call("blade_beamform_detect_tc", ptr(xd), ptr(plan), ptr(od2), B, A, F, T, 2, R, I, stream())
+    np.testing.assert_array_equal(host(od2), y)
+
+
+def test_tensor_core_matches_fp32_path(cuda):
+    A, F, T, B, R, I = 28, 8, 2048, 16, 4, 4
+    x, w = make(A, F, T, B, 3)
+    xd, wd = dev(x), c64(w)
+    lib = _lib.load()
+    plan = torch.empty(int(lib.blade_beamform_tc_plan_size(B, A, F, 2)), dtype=torch.uint8, device="cuda")
+    o1 = torch.zeros((B, F * R, T // (R * I), 1), dtype=torch.float32, device="cuda")
+    o2 = torch.zeros_like(o1)
+    call("blade_beamform_tc_prepare", ptr(wd), ptr(plan), B, A, F, 2, stream())
+    call("blade_beamform_detect_tc", ptr(xd), ptr(plan), ptr(o1), B, A, F, T, 2, R, I, stream())
+    call("blade_beamform_detect_f32", _lib.CI8, ptr(xd), ptr(wd), ptr(o2), B, A, F, T, 2, R, I, stream())
+    assert rel_l2(host(o1), host(o2)) < 2 * TOL
+
+
+def test_unfused_module_chain_matches_fused(cuda):
+    # Cast -> Beamformer -> Channelizer -> Detector as four modules (the reference's
+    # ModeB order) equals the fused kernels.
+    A, F, T, B, R, I = 20, 6, 1024, 8, 4, 4
+    x, w = make(A, F, T, B, 4)
+    xd = bl.array_tensor((A, F, T, 2), dtype=bl.ci8)
+    xd.as_torch().copy_(dev(x))
+    wd = bl.phasor_tensor((B, A, F, 1, 2), dtype=bl.cf32)
+    wd.as_torch().copy_(c64(w))
+    cast = bl.module(bl.cast, {}, xd, it=bl.ci8, ot=bl.cf32)
+    bf = bl.module(bl.beamformer, {}, (cast.get_output(), wd), telescope=bl.ata)
+    ch = bl.module(bl.channelizer, {"rate": R}, bf.get_output())
+    det = bl.module(bl.detector, {"integration_size": I, "number_of_output_polarizations": 1}, ch.get_output())
+    for m in (cast, bf, ch, det):
+        assert m.process(0) == bl.result.success
+    fused = bl.module(bl.beamform_detect, {"rate": R, "integration_size": I}, (xd, wd), telescope=bl.ata)
+    fused.process(0)
+    torch.cuda.synchronize()
+    ref = O.beamform_channelize_detect(x, w, R, I)
+    assert rel_l2(det.get_output().as_torch().cpu().numpy(), ref) < TOL
+    assert rel_l2(fused.get_output().as_torch().cpu().numpy(), ref) < TOL
+    assert fused.precision == "fp16_split"
+
+
+# ------------------------------------------------------------------------ adjoint
+@pytest.mark.parametrize("A,F,T,B", [(28, 6, 2048, 1), (7, 3, 300, 3), (16, 2, 512, 20)])
+def test_adjoint_gradient_vs_fp64(cuda, A, F, T, B):
+    rng = np.random.default_rng(A + B)
+    x, _ = S.calibration_voltages(rng, A, F, T)
+    w = (rng.standard_normal((B, A, F, 1, 2)) + 1j * rng.standard_normal((B, A, F, 1, 2))) / np.sqrt(A)
+    xd, wd = c64(x), c64(w)
+    gd = torch.zeros((B, A, F, 1, 2), dtype=torch.complex64, device="cuda")
+    ld = torch.zeros(F * 2, dtype=torch.float64, device="cuda")
+    call("blade_beamform_detect_adjoint", ptr(xd), ptr(wd), ptr(gd), ptr(ld), B, A, F, T, 2, stream())
+    x32, w32 = x.astype(np.complex64), w.astype(np.complex64)
+    g_ref = O.stokes_loss_grad(x32, w32)
+    assert rel_l2(host(gd), g_ref) < TOL
+    assert abs(host(ld).sum() - O.stokes_loss(x32, w32)) / abs(O.stokes_loss(x32, w32)) < TOL
