@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(kT) adjoint_kernel(const float2* __restrict__ 
     double lsum = 0.0;
     // Thread split of the pair reduction: S slices of the tile per pair.
     const uint32_t S = Q >= kT ? 1 : kT / Q;
-    const uint32_t span = kT / S;
+    const uint32_t span = (kT + S - 1) / S;  // the S slices cover every sample of the tile
     __syncthreads();
 
     for (uint32_t t0 = 0; t0 < T; t0 += kT) {
@@ -78,7 +78,8 @@ __global__ void __launch_bounds__(kT) adjoint_kernel(const float2* __restrict__ 
             float2 part = make_float2(0.f, 0.f);
             if (q < Q && sl < S) {
                 const uint32_t b = q / A, a = q % A;
-                for (uint32_t t = sl * span; t < (sl + 1) * span; t++) {
+                const uint32_t t_end = min((sl + 1) * span, (uint32_t)kT);
+                for (uint32_t t = sl * span; t < t_end; t++) {
                     const float2 yv = ys[b * kT + t], xv = xs[a * kT + t];
                     part.x = fmaf(yv.x, xv.x, part.x);
                     part.x = fmaf(yv.y, xv.y, part.x);
