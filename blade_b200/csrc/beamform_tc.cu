@@ -37,6 +37,8 @@
 // (full/empty), phasor image (full/empty).  Every wait is bounded (clock budget
 // plus a shared abort flag); on expiry the kernel records a status word, drains
 // its own MMAs and bulk copies, frees TMEM and returns.
+#include <mutex>
+
 #include "common.cuh"
 #include "tc_ptx.cuh"
 
@@ -525,4 +527,62 @@ extern "C" int blade_device_status(uint32_t* status) {
     if (e != cudaSuccess) return check_cuda(e, "blade_device_status");
     if (status) *status = v;
     return BLADE_SUCCESS;
+}
+
+// ---- allocation-free variant ---------------------------------------------------
+// For callers that must not allocate device memory while they stream: an online
+// beamformer that sizes its whole GPU budget once at start-up and then runs a
+// fixed-cadence loop cannot call cudaMalloc / cudaFree per block, because those
+// calls synchronise the device and take unbounded time, which the loop's
+// real-time deadline cannot absorb.  This entry point keeps the phasor image in a
+// fixed device array that every GPU loading the library holds until exit.
+
+// Scratch for the phasor image: 8 MiB per device.
+static __device__ __align__(256) uint8_t g_tc_noalloc_plan[8u << 20];
+
+namespace {
+
+constexpr uint64_t kNoAllocPlanBytes = 8ull << 20;
+
+// Device address of g_tc_noalloc_plan, looked up once per device with that device
+// current (the host-side name is only a stand-in for the device array).
+int noalloc_plan_address(void** out) {
+    static std::mutex mu;
+    static void* addr[64] = {nullptr};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return check_cuda(e, "blade_beamform_detect_tc_noalloc");
+    if (dev < 0 || dev >= 64) return set_error(BLADE_ERROR, "blade_beamform_detect_tc_noalloc: device %d", dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_tc_noalloc_plan);
+        if (e != cudaSuccess) return check_cuda(e, "blade_beamform_detect_tc_noalloc: cudaGetSymbolAddress");
+        addr[dev] = p;
+    }
+    *out = addr[dev];
+    return BLADE_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" int blade_beamform_detect_tc_noalloc(const void* in, const void* phasors, void* out, uint64_t B,
+                                                uint64_t A, uint64_t F, uint64_t T, uint64_t P, uint64_t rate,
+                                                uint64_t integration, blade_stream_t stream) {
+    if (!blade_beamform_detect_tc_supported(B, A, F, T, P, rate, integration))
+        return set_error(BLADE_ERROR,
+                         "blade_beamform_detect_tc_noalloc: unsupported configuration (needs P=2, 1<=A<=64, "
+                         "T%%128==0, rate in {1,2,4}, I a power of two <= 32)");
+    const uint64_t need = blade_beamform_tc_plan_size(B, A, F, P);
+    if (need > kNoAllocPlanBytes)
+        return set_error(BLADE_ERROR,
+                         "blade_beamform_detect_tc_noalloc: the phasor image for B=%llu A=%llu F=%llu needs %llu "
+                         "bytes, above the %llu-byte static workspace; use blade_beamform_tc_prepare + "
+                         "blade_beamform_detect_tc with a caller-allocated image",
+                         (unsigned long long)B, (unsigned long long)A, (unsigned long long)F,
+                         (unsigned long long)need, (unsigned long long)kNoAllocPlanBytes);
+    void* plan = nullptr;
+    if (int rc = noalloc_plan_address(&plan)) return rc;
+    if (int rc = blade_beamform_tc_prepare(phasors, plan, B, A, F, P, stream)) return rc;
+    return blade_beamform_detect_tc(in, plan, out, B, A, F, T, P, rate, integration, stream);
 }

@@ -211,6 +211,27 @@ BLADE_API int blade_beamform_detect_tc(const void* in, const void* plan, void* o
 BLADE_API int blade_device_status(uint32_t* status);
 
 /* ---------------------------------------------------------------------------
+ * Allocation-free tensor-core chain (no counterpart in the reference).
+ * Same computation, arguments and output as blade_beamform_tc_prepare followed
+ * by blade_beamform_detect_tc, but the phasor image lives in a fixed 8 MiB
+ * device array inside this library instead of caller-allocated memory, so the
+ * call itself allocates nothing (no cudaMalloc / cudaFree).  It is meant for
+ * streaming callers whose device memory is sized once at start-up and whose
+ * fixed-cadence loop cannot absorb the device synchronisation of an allocation.
+ * Limit: blade_beamform_tc_plan_size(B, A, F, P) <= 8 MiB (e.g. A <= 32,
+ * B <= 16 up to 682 channels); larger images are rejected with BLADE_ERROR.
+ * The first call on each device looks up the array's device address (make that
+ * first call before any stream capture).  All calls share the one array: calls
+ * that overlap on the GPU (different streams, or different host threads) race;
+ * serialise them on one stream.  Each call rewrites the whole image it uses.
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_beamform_detect_tc_noalloc(const void* in, const void* phasors,
+                                               void* out, uint64_t B, uint64_t A,
+                                               uint64_t F, uint64_t T, uint64_t P,
+                                               uint64_t rate, uint64_t integration,
+                                               blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Adjoint of beamform + Stokes-I detect (no reference counterpart).
  * For L = -sum_{b,f,t,p} |y[b,f,t,p]|^2, y = beamform(in, phasors):
  *   grad[b,a,f,0,p] = dL/d conj(w) = -sum_t y[b,f,t,p] conj(in[a,f,t,p])
