@@ -28,15 +28,18 @@
 //
 // CTA organisation (persistent, one CTA per SM, 14 warps):
 //   warp 0      TMEM allocation; lane 0 issues tcgen05.mma and commits
-//   warp 1      lane 0 loads the per-channel phasor image with one bulk copy
+//   warp 1      loader: the per-channel phasor image (one bulk copy) and the raw
+//               CI8 tiles (one 512-byte bulk copy per antenna row, all lanes),
+//               into a ring of raw stages several tiles ahead
 //   warps 2-5   epilogue: tcgen05.ld of the accumulators, |.|^2 over both
 //               polarisations, window sums with lane shuffles, Stokes-I stores
-//   warps 6-13  operand build: CI8 loads, DFT, exact int8 -> FP16 conversion,
-//               stores in the UMMA core-matrix layout
-// Pipelines: operand stages (full/empty mbarriers), two TMEM accumulator buffers
-// (full/empty), phasor image (full/empty).  Every wait is bounded (clock budget
-// plus a shared abort flag); on expiry the kernel records a status word, drains
-// its own MMAs and bulk copies, frees TMEM and returns.
+//   warps 6-13  operand build from the raw ring: DFT, exact int8 -> FP16
+//               conversion, stores in the UMMA core-matrix layout, one
+//               polarisation per operand stage
+// Pipelines (full/empty mbarrier pairs): raw stages, operand stages (one per tile
+// and polarisation), two TMEM accumulator buffers, the phasor image.  Every wait
+// is bounded (clock budget plus a shared abort flag); on expiry the kernel records
+// a status word, drains its own MMAs and bulk copies, frees TMEM and returns.
 #include <mutex>
 
 #include "common.cuh"
@@ -64,9 +67,9 @@ struct TcArgs {
     const uint8_t* in;    // CI8 [A, F, T, 2]
     const uint8_t* plan;  // phasor images, one per channel, img_bytes each
     float* out;           // [beams, F*R, U]
-    uint32_t A, F, T, beams, U, integ;
-    uint32_t NB, KA, stages;
-    uint32_t img_bytes, tiles_per_ch;
+    uint32_t A, F, T, beams, U;
+    uint32_t NB, KA, a_stages, r_stages;
+    uint32_t img_bytes, raw_bytes, tiles_per_ch;
     uint64_t total_tiles;
 };
 
@@ -88,9 +91,11 @@ __device__ __forceinline__ half2 sample_h2(uint32_t w, int p) {
 
 __device__ __forceinline__ uint32_t h2u(half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
 
-// Byte offset of element (row, k) inside an operand block with K extent KA.
-__device__ __forceinline__ uint32_t cm_off(uint32_t row, uint32_t kchunk, uint32_t KA) {
-    return (row >> 3) * (16u * KA) + kchunk * 128u + (row & 7u) * 16u;
+// Address of K element k_total (a multiple of 4) of row `row` in one
+// polarisation's operand: Xr occupies k_total in [0, KA), Xi [KA, 2 KA); every
+// 64 K elements form one 128-row x 128-byte swizzled block of 16 KB.
+__device__ __forceinline__ uint32_t op_off(uint32_t row, uint32_t k_total) {
+    return (k_total >> 6) * 16384u + sw128_off(row, (k_total >> 3) & 7u) + ((k_total & 4u) << 1);
 }
 
 __device__ __forceinline__ void record_abort(volatile int* abort, unsigned code) {
@@ -98,18 +103,171 @@ __device__ __forceinline__ void record_abort(volatile int* abort, unsigned code)
     atomicCAS(&g_tc_status, 0u, code);
 }
 
+// rate-4 spectrum of one antenna and polarisation from its 4 sample words:
+// Z[k] = sum_j (-1)^j x_j e^{-2 pi i j k / 4}, exact in FP16 (|Z| <= 512).
+__device__ __forceinline__ void dft4_h2(uint4 v, int p, half2 (&Z)[4]) {
+    const half2 x0 = sample_h2(v.x, p), x1 = sample_h2(v.y, p), x2 = sample_h2(v.z, p), x3 = sample_h2(v.w, p);
+    const half2 e02 = __hadd2(x0, x2), d02 = __hsub2(x0, x2);
+    const half2 e13 = __hadd2(x1, x3), d13 = __hsub2(x1, x3);
+    const half2 id13 = __hmul2(__lowhigh2highlow(d13), __halves2half2(__float2half(-1.f), __float2half(1.f)));
+    Z[0] = __hsub2(e02, e13);  // x0 - x1 + x2 - x3
+    Z[1] = __hadd2(d02, id13); // x0 + i x1 - x2 - i x3
+    Z[2] = __hadd2(e02, e13);  // x0 + x1 + x2 + x3
+    Z[3] = __hsub2(d02, id13); // x0 - i x1 - x2 + i x3
+}
+
+// R = 1 operand chunk: 8 antennas of one sample -> (re, im) chunks of polarisation p.
+__device__ __forceinline__ void r1_chunks(const uint32_t (&w)[8], int p, uint4& vr, uint4& vi) {
+    const uint32_t sre = p ? 0x0602u : 0x0400u, sim = p ? 0x0703u : 0x0501u;
+    vr.x = cvt_pair(__byte_perm(w[0], w[1], sre));
+    vr.y = cvt_pair(__byte_perm(w[2], w[3], sre));
+    vr.z = cvt_pair(__byte_perm(w[4], w[5], sre));
+    vr.w = cvt_pair(__byte_perm(w[6], w[7], sre));
+    vi.x = cvt_pair(__byte_perm(w[0], w[1], sim));
+    vi.y = cvt_pair(__byte_perm(w[2], w[3], sim));
+    vi.z = cvt_pair(__byte_perm(w[4], w[5], sim));
+    vi.w = cvt_pair(__byte_perm(w[6], w[7], sim));
+}
+
+// Builds the operand rows of polarisation p for one tile from the raw tile in
+// shared memory (antenna-major, 512 bytes = 128 samples x 4 bytes per antenna).
+// Row = k * (128 / R) + spectrum.  Consecutive lanes take consecutive rows, so
+// every 16-byte store of a warp lands in a distinct bank group of the swizzle.
 template <int R>
+__device__ __forceinline__ void build_operand(const uint8_t* raw, uint8_t* op, uint32_t A, uint32_t KA, int p,
+                                              uint32_t ct) {
+    constexpr uint32_t kStride = kConvWarps * 32;
+    if constexpr (R == 1) {
+        const uint32_t ntasks = kM * (KA / 8);
+        // Two tasks per pass: both tasks' shared-memory loads are in flight together.
+        for (uint32_t t0 = ct; t0 < ntasks; t0 += 2 * kStride) {
+            const uint32_t t1 = t0 + kStride;
+            const bool has1 = t1 < ntasks;
+            const uint32_t s0 = t0 % kM, g0 = t0 / kM, s1 = t1 % kM, g1 = t1 / kM;
+            uint32_t w0[8], w1[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const uint32_t a0 = g0 * 8 + i, a1 = g1 * 8 + i;
+                w0[i] = a0 < A ? *reinterpret_cast<const uint32_t*>(raw + a0 * 512 + s0 * 4) : 0u;
+                w1[i] = (has1 && a1 < A) ? *reinterpret_cast<const uint32_t*>(raw + a1 * 512 + s1 * 4) : 0u;
+            }
+            uint4 vr, vi;
+            r1_chunks(w0, p, vr, vi);
+            *reinterpret_cast<uint4*>(op + op_off(s0, g0 * 8)) = vr;
+            *reinterpret_cast<uint4*>(op + op_off(s0, KA + g0 * 8)) = vi;
+            if (has1) {
+                r1_chunks(w1, p, vr, vi);
+                *reinterpret_cast<uint4*>(op + op_off(s1, g1 * 8)) = vr;
+                *reinterpret_cast<uint4*>(op + op_off(s1, KA + g1 * 8)) = vi;
+            }
+        }
+    } else if constexpr (R == 2) {
+        const uint32_t ntasks = (kM / 2) * (KA / 8);
+        for (uint32_t task = ct; task < ntasks; task += kStride) {
+            const uint32_t s = task % (kM / 2), grp = task / (kM / 2);
+            uint2 v[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const uint32_t a = grp * 8 + i;
+                v[i] = a < A ? *reinterpret_cast<const uint2*>(raw + a * 512 + s * 8) : make_uint2(0u, 0u);
+            }
+            half2 Z0[8], Z1[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const half2 x0 = sample_h2(v[i].x, p), x1 = sample_h2(v[i].y, p);
+                Z0[i] = __hsub2(x0, x1);  // k = 0: x0 - x1
+                Z1[i] = __hadd2(x0, x1);  // k = 1: x0 + x1
+            }
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const half2* Z = k ? Z1 : Z0;
+                uint4 vr, vi;
+                vr.x = __byte_perm(h2u(Z[0]), h2u(Z[1]), 0x5410);
+                vr.y = __byte_perm(h2u(Z[2]), h2u(Z[3]), 0x5410);
+                vr.z = __byte_perm(h2u(Z[4]), h2u(Z[5]), 0x5410);
+                vr.w = __byte_perm(h2u(Z[6]), h2u(Z[7]), 0x5410);
+                vi.x = __byte_perm(h2u(Z[0]), h2u(Z[1]), 0x7632);
+                vi.y = __byte_perm(h2u(Z[2]), h2u(Z[3]), 0x7632);
+                vi.z = __byte_perm(h2u(Z[4]), h2u(Z[5]), 0x7632);
+                vi.w = __byte_perm(h2u(Z[6]), h2u(Z[7]), 0x7632);
+                const uint32_t row = k * (kM / 2) + s;
+                *reinterpret_cast<uint4*>(op + op_off(row, grp * 8)) = vr;
+                *reinterpret_cast<uint4*>(op + op_off(row, KA + grp * 8)) = vi;
+            }
+        }
+    } else {
+        // R == 4: a task is one spectrum of 4 antennas (half a K chunk, 8-byte stores).
+        const uint32_t ntasks = (kM / 4) * (KA / 4);
+        for (uint32_t task = ct; task < ntasks; task += kStride) {
+            const uint32_t s = task % (kM / 4), g4 = task / (kM / 4);
+            uint4 v[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint32_t a = g4 * 4 + i;
+                v[i] = a < A ? *reinterpret_cast<const uint4*>(raw + a * 512 + s * 16) : make_uint4(0u, 0u, 0u, 0u);
+            }
+            half2 Z[4][4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) dft4_h2(v[i], p, Z[i]);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                uint2 vr, vi;
+                vr.x = __byte_perm(h2u(Z[0][k]), h2u(Z[1][k]), 0x5410);
+                vr.y = __byte_perm(h2u(Z[2][k]), h2u(Z[3][k]), 0x5410);
+                vi.x = __byte_perm(h2u(Z[0][k]), h2u(Z[1][k]), 0x7632);
+                vi.y = __byte_perm(h2u(Z[2][k]), h2u(Z[3][k]), 0x7632);
+                const uint32_t row = k * (kM / 4) + s;
+                *reinterpret_cast<uint2*>(op + op_off(row, g4 * 4)) = vr;
+                *reinterpret_cast<uint2*>(op + op_off(row, KA + g4 * 4)) = vi;
+            }
+        }
+    }
+}
+
+// Window sum of 16 per-beam values over I = 2^LOGI adjacent lanes by a butterfly
+// reduce-scatter: after min(LOGI, 4) halving rounds each lane holds the window sums
+// of 16 >> min(LOGI, 4) consecutive beams starting at *first; the rest of the
+// rounds (I = 32) are a plain exchange.  Returns the number of values this lane
+// stores (0 for the duplicate half when I = 32).
+template <int LOGI>
+__device__ __forceinline__ int window_reduce(float (&v)[16], uint32_t lane, uint32_t* first) {
+    constexpr int RS = LOGI < 4 ? LOGI : 4;
+    uint32_t off = 0;
+#pragma unroll
+    for (int s = 0; s < RS; s++) {
+        const int half = 16 >> (s + 1);
+        const bool upper = (lane >> s) & 1u;
+#pragma unroll
+        for (int j = 0; j < half; j++) {
+            const float send = upper ? v[j] : v[half + j];
+            const float recv = __shfl_xor_sync(0xffffffffu, send, 1 << s);
+            v[j] = (upper ? v[half + j] : v[j]) + recv;
+        }
+        if (upper) off += half;
+    }
+#pragma unroll
+    for (int s = RS; s < LOGI; s++) v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1 << s);
+    *first = off;
+    if (LOGI > 4 && ((lane >> 4) & 1u)) return 0;
+    return 16 >> RS;
+}
+
+template <int R, int LOGI>
 __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g) {
-    extern __shared__ __align__(1024) uint8_t smem[];
-    const uint32_t NB = g.NB, KA = g.KA, S = g.stages;
-    const uint32_t blkW = NB * KA * 2;      // one [NB x KA] fp16 block
-    const uint32_t blkA = kM * KA * 2;      // one [128 x KA] fp16 block
-    uint8_t* w_smem = smem;                 // 12 blocks: [p][h][-Wi | Wr | Wi]
-    uint8_t* a_smem = smem + 12 * blkW;     // S stages x 4 blocks: [p][Xr | Xi]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(a_smem + (size_t)S * 4 * blkA);
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    // Swizzled operands need 1024-byte aligned atoms: align the working base.
+    uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    const uint32_t NB = g.NB, KA = g.KA, AS = g.a_stages, RS = g.r_stages;
+    const uint32_t op_bytes = (2 * KA / 64) * 16384u;  // one polarisation's operand
+    uint8_t* w_smem = smem;                              // phasor image
+    uint8_t* a_smem = w_smem + g.img_bytes;              // AS operand stages
+    uint8_t* r_smem = a_smem + (size_t)AS * op_bytes;    // RS raw tiles
+    uint64_t* bars = reinterpret_cast<uint64_t*>(r_smem + (size_t)RS * g.raw_bytes);
     uint64_t* a_full = bars;
-    uint64_t* a_empty = bars + S;
-    uint64_t* d_full = bars + 2 * S;
+    uint64_t* a_empty = a_full + AS;
+    uint64_t* r_full = a_empty + AS;
+    uint64_t* r_empty = r_full + RS;
+    uint64_t* d_full = r_empty + RS;
     uint64_t* d_empty = d_full + 2;
     uint64_t* w_full = d_empty + 2;
     uint64_t* w_empty = w_full + 1;
@@ -122,9 +280,13 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g) {
     const uint32_t tmem_cols = (8 * NB <= 32) ? 32 : (8 * NB <= 64) ? 64 : (8 * NB <= 128) ? 128 : (8 * NB <= 256) ? 256 : 512;
 
     if (threadIdx.x == 0) {
-        for (uint32_t i = 0; i < S; i++) {
+        for (uint32_t i = 0; i < AS; i++) {
             mbar_init(&a_full[i], kConvWarps);
             mbar_init(&a_empty[i], 1);
+        }
+        for (uint32_t i = 0; i < RS; i++) {
+            mbar_init(&r_full[i], 1);
+            mbar_init(&r_empty[i], kConvWarps);
         }
         for (int i = 0; i < 2; i++) {
             mbar_init(&d_full[i], 1);
@@ -155,43 +317,45 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g) {
         // ---------------- MMA issuer ----------------
         if (lane == 0 && L0 < L1) {
             const uint32_t idesc = idesc_f16(kM, 2 * NB);
-            const uint32_t sbo = 16 * KA;
             const uint32_t w_base = smem_u32(w_smem), a_base = smem_u32(a_smem);
-            uint32_t st = 0, aph = 0, db = 0, dph = 0, wph = 0;
+            const uint32_t ksteps = 2 * KA / 16;
+            // Phasor image per (p, h): KA = 64 -> blocks [-Wi | Wr | Wi] of NB rows;
+            // KA = 32 -> one block of 2 NB rows ([Wr | -Wi] over [Wi | Wr]).
+            const uint32_t ph_bytes = (KA == 64 ? 3u : 2u) * NB * 128u;
+            uint32_t as = 0, aph = 0, db = 0, dph = 0, wph = 0;
             bool ok = true;
             for (uint64_t L = L0; L < L1 && ok; L++) {
                 const uint32_t tt = (uint32_t)(L % tpc);
                 if (L == L0 || tt == 0) {
                     if (!mbar_wait(w_full, wph, abort, kWaitBudget)) { record_abort(abort, 1); ok = false; break; }
                 }
-                if (!mbar_wait(&a_full[st], aph, abort, kWaitBudget)) { record_abort(abort, 2); ok = false; break; }
                 if (!mbar_wait(&d_empty[db], dph ^ 1, abort, kWaitBudget)) { record_abort(abort, 3); ok = false; break; }
-                tc_fence_after();
-                const uint32_t a_stage = a_base + st * 4 * blkA;
                 for (uint32_t p = 0; p < 2; p++) {
+                    if (!mbar_wait(&a_full[as], aph, abort, kWaitBudget)) { record_abort(abort, 2); ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t a_stage = a_base + as * op_bytes;
                     const uint32_t d = tmem + db * (4 * NB) + p * (2 * NB);
                     uint32_t acc = 0;
                     for (uint32_t h = 0; h < 2; h++) {
-                        const uint32_t wblk = w_base + (p * 2 + h) * 3 * blkW;
-                        for (uint32_t ri = 0; ri < 2; ri++) {
-                            const uint32_t abase = a_stage + (p * 2 + ri) * blkA;
-                            const uint32_t bbase = wblk + (ri == 0 ? 1 : 0) * blkW;
-                            for (uint32_t ks = 0; ks < KA / 16; ks++) {
-                                const uint64_t ad = smem_desc(abase + ks * 256, 128, sbo);
-                                const uint64_t bd = smem_desc(bbase + ks * 256, 128, sbo);
-                                mma_f16(d, ad, bd, idesc, acc);
-                                acc = 1;
-                            }
+                        const uint32_t wph_base = w_base + (p * 2 + h) * ph_bytes;
+                        for (uint32_t j = 0; j < ksteps; j++) {
+                            const uint32_t aaddr = a_stage + (j >> 2) * 16384u + (j & 3u) * 32u;
+                            uint32_t baddr;
+                            if (KA == 64) baddr = wph_base + (j < 4 ? NB * 128u : 0u) + (j & 3u) * 32u;
+                            else baddr = wph_base + j * 32u;
+                            mma_f16(d, smem_desc_sw128(aaddr), smem_desc_sw128(baddr), idesc, acc);
+                            acc = 1;
                         }
                     }
+                    mma_commit(&a_empty[as]);
+                    if (++as == AS) { as = 0; aph ^= 1; }
                 }
-                mma_commit(&a_empty[st]);
+                if (!ok) break;
                 mma_commit(&d_full[db]);
                 if (tt == tpc - 1 || L + 1 == L1) {
                     mma_commit(w_empty);
                     wph ^= 1;
                 }
-                if (++st == S) { st = 0; aph ^= 1; }
                 if (++db == 2) { db = 0; dph ^= 1; }
             }
             // Drain every MMA issued by this thread before TMEM is released
@@ -200,32 +364,61 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g) {
             if (!mbar_wait(fin, 0, &never, kWaitBudget)) record_abort(abort, 4);
         }
     } else if (warp == 1) {
-        // ---------------- phasor image loader ----------------
-        if (lane == 0 && L0 < L1) {
-            uint32_t wph = 0;
-            bool issued = false;
+        // ---------------- loader: phasor image + raw CI8 tiles (bulk copies) ----------------
+        if (L0 < L1) {
+            uint32_t rs = 0, rph = 0, wph = 0;
+            bool w_issued = false;
+            uint32_t issued_mask = 0, issued_par = 0;  // per raw stage: issued?, parity of last issue
             for (uint64_t L = L0; L < L1; L++) {
-                const uint32_t tt = (uint32_t)(L % tpc);
-                if (!(L == L0 || tt == 0)) continue;
-                if (!mbar_wait(w_empty, wph ^ 1, abort, kWaitBudget)) { record_abort(abort, 5); break; }
-                const uint32_t f = (uint32_t)(L / tpc);
-                mbar_arrive_expect_tx(w_full, g.img_bytes);
-                bulk_g2s(w_smem, g.plan + (uint64_t)f * g.img_bytes, g.img_bytes, w_full);
-                issued = true;
-                wph ^= 1;
+                const uint32_t f = (uint32_t)(L / tpc), tt = (uint32_t)(L % tpc);
+                int ok = 1;
+                if (L == L0 || tt == 0) {
+                    if (lane == 0) {
+                        ok = mbar_wait(w_empty, wph ^ 1, abort, kWaitBudget);
+                        if (ok) {
+                            mbar_arrive_expect_tx(w_full, g.img_bytes);
+                            bulk_g2s(w_smem, g.plan + (uint64_t)f * g.img_bytes, g.img_bytes, w_full);
+                        } else {
+                            record_abort(abort, 5);
+                        }
+                    }
+                    ok = __shfl_sync(0xffffffffu, ok, 0);
+                    if (!ok) break;
+                    w_issued = true;
+                    wph ^= 1;
+                }
+                if (lane == 0) {
+                    ok = mbar_wait(&r_empty[rs], rph ^ 1, abort, kWaitBudget);
+                    if (ok) mbar_arrive_expect_tx(&r_full[rs], g.A * 512u);
+                    else record_abort(abort, 9);
+                }
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                if (!ok) break;
+                uint8_t* dst = r_smem + (size_t)rs * g.raw_bytes;
+                const uint8_t* src = g.in + ((uint64_t)f * g.T + (uint64_t)tt * kM) * 4;
+                for (uint32_t a = lane; a < g.A; a += 32)
+                    bulk_g2s(dst + a * 512, src + (uint64_t)a * g.F * g.T * 4, 512, &r_full[rs]);
+                issued_mask |= 1u << rs;
+                issued_par = (issued_par & ~(1u << rs)) | (rph << rs);
+                if (++rs == RS) { rs = 0; rph ^= 1; }
             }
-            // The last copy must land before the CTA exits.
-            if (issued && !mbar_wait(w_full, wph ^ 1, &never, kWaitBudget)) record_abort(abort, 6);
+            // Every bulk copy this warp issued must land before the CTA exits.
+            if (lane == 0) {
+                if (w_issued && !mbar_wait(w_full, wph ^ 1, &never, kWaitBudget)) record_abort(abort, 6);
+                for (uint32_t s = 0; s < RS; s++)
+                    if ((issued_mask >> s) & 1u)
+                        if (!mbar_wait(&r_full[s], (issued_par >> s) & 1u, &never, kWaitBudget)) record_abort(abort, 10);
+            }
+            __syncwarp();
         }
     } else if (warp < 2 + kEpiWarps) {
         // ---------------- epilogue ----------------
+        constexpr uint32_t I = 1u << LOGI;
         const uint32_t q = warp & 3;  // TMEM lane quarter this warp may access
-        const uint32_t rows_per_k = kM / R;
+        constexpr uint32_t rows_per_k = kM / R;
         const uint32_t row = 32 * q + lane;
         const uint32_t k = row / rows_per_k;
         const uint32_t s_local = row - k * rows_per_k;
-        const uint32_t I = g.integ;
-        const bool leader = (lane % I) == 0;
         uint32_t db = 0, dph = 0;
         for (uint64_t L = L0; L < L1; L++) {
             if (!mbar_wait(&d_full[db], dph, abort, kWaitBudget)) { record_abort(abort, 7); break; }
@@ -233,31 +426,29 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g) {
             const uint32_t f = (uint32_t)(L / tpc), tt = (uint32_t)(L % tpc);
             const uint32_t u = (tt * rows_per_k + s_local) / I;
             const uint32_t lane_addr = tmem + ((32 * q) << 16) + db * (4 * NB);
+            float* obase = g.out + ((uint64_t)f * R + k) * g.U + u;
+            const uint64_t bstride = (uint64_t)g.F * R * g.U;
             for (uint32_t bc = 0; bc < NB; bc += 16) {
+                uint32_t r0[16], i0[16], r1[16], i1[16];
+                tmem_ld16(lane_addr + bc, r0);
+                tmem_ld16(lane_addr + NB + bc, i0);
+                tmem_ld16(lane_addr + 2 * NB + bc, r1);
+                tmem_ld16(lane_addr + 3 * NB + bc, i1);
+                tmem_ld_wait();
                 float pw[16];
 #pragma unroll
-                for (int j = 0; j < 16; j++) pw[j] = 0.f;
-#pragma unroll
-                for (uint32_t p = 0; p < 2; p++) {
-                    uint32_t re[16], im[16];
-                    tmem_ld16(lane_addr + p * (2 * NB) + bc, re);
-                    tmem_ld16(lane_addr + p * (2 * NB) + NB + bc, im);
-                    tmem_ld_wait();
-#pragma unroll
-                    for (int j = 0; j < 16; j++) {
-                        const float a = __uint_as_float(re[j]), b = __uint_as_float(im[j]);
-                        pw[j] = fmaf(a, a, fmaf(b, b, pw[j]));
-                    }
+                for (int j = 0; j < 16; j++) {
+                    const float a0 = __uint_as_float(r0[j]), b0 = __uint_as_float(i0[j]);
+                    const float a1 = __uint_as_float(r1[j]), b1 = __uint_as_float(i1[j]);
+                    pw[j] = fmaf(a0, a0, fmaf(b0, b0, fmaf(a1, a1, b1 * b1)));
                 }
-                for (uint32_t o = 1; o < I; o <<= 1) {
+                uint32_t first;
+                const int cnt = window_reduce<LOGI>(pw, lane, &first);
 #pragma unroll
-                    for (int j = 0; j < 16; j++) pw[j] += __shfl_xor_sync(0xffffffffu, pw[j], o);
-                }
-                if (leader) {
-#pragma unroll
-                    for (int j = 0; j < 16; j++) {
-                        const uint32_t b = bc + j;
-                        if (b < g.beams) g.out[((uint64_t)(b * (uint64_t)g.F + f) * R + k) * g.U + u] = pw[j];
+                for (int j = 0; j < 16; j++) {
+                    if (j < cnt) {
+                        const uint32_t b = bc + first + j;
+                        if (b < g.beams) obase[b * bstride] = pw[j];
                     }
                 }
             }
@@ -269,91 +460,23 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g) {
     } else {
         // ---------------- operand build ----------------
         const uint32_t ct = threadIdx.x - (2 + kEpiWarps) * 32;  // 0..255
-        const uint32_t spectra = kM / R;
-        const uint32_t groups = KA / 8;
-        const uint32_t ntasks = spectra * groups;
-        const uint64_t ch_stride = (uint64_t)g.T * 4;  // bytes between (a, f) rows... per channel
-        uint32_t st = 0, aph = 0;
-        for (uint64_t L = L0; L < L1; L++) {
-            if (!mbar_wait(&a_empty[st], aph ^ 1, abort, kWaitBudget)) { record_abort(abort, 8); break; }
-            const uint32_t f = (uint32_t)(L / tpc), tt = (uint32_t)(L % tpc);
-            uint8_t* stage = a_smem + (size_t)st * 4 * blkA;
-            for (uint32_t task = ct; task < ntasks; task += kConvWarps * 32) {
-                const uint32_t s = task % spectra, grp = task / spectra;
-                const uint32_t t = tt * kM + s * R;
-                // Raw samples: [antenna][R samples], one 32-bit word per sample.
-                uint32_t raw[8][R];
-#pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    const uint32_t a = grp * 8 + i;
-                    if (a < g.A) {
-                        const uint8_t* src = g.in + ((uint64_t)a * g.F + f) * ch_stride + (uint64_t)t * 4;
-                        if (R == 4) {
-                            uint4 v = ldg_nc_u4(src);
-                            raw[i][0] = v.x;
-                            raw[i][R > 1 ? 1 : 0] = v.y;
-                            raw[i][R > 2 ? 2 : 0] = v.z;
-                            raw[i][R > 3 ? 3 : 0] = v.w;
-                        } else if (R == 2) {
-                            uint2 v = __ldg(reinterpret_cast<const uint2*>(src));
-                            raw[i][0] = v.x;
-                            raw[i][R > 1 ? 1 : 0] = v.y;
-                        } else {
-                            raw[i][0] = __ldg(reinterpret_cast<const uint32_t*>(src));
-                        }
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < R; j++) raw[i][j] = 0u;
-                    }
-                }
-#pragma unroll
-                for (int p = 0; p < 2; p++) {
-                    // Z[i][k] = (re, im) half2 of fine channel k for antenna 8 grp + i.
-                    half2 Z[8][R];
-#pragma unroll
-                    for (int i = 0; i < 8; i++) {
-                        if (R == 1) {
-                            Z[i][0] = sample_h2(raw[i][0], p);
-                        } else if (R == 2) {
-                            const half2 x0 = sample_h2(raw[i][0], p), x1 = sample_h2(raw[i][R - 1], p);
-                            Z[i][0] = __hsub2(x0, x1);       // k = 0: x0 - x1
-                            Z[i][R - 1] = __hadd2(x0, x1);   // k = 1: x0 + x1
-                        } else {
-                            const half2 x0 = sample_h2(raw[i][0], p), x1 = sample_h2(raw[i][R > 1 ? 1 : 0], p);
-                            const half2 x2 = sample_h2(raw[i][R > 2 ? 2 : 0], p), x3 = sample_h2(raw[i][R > 3 ? 3 : 0], p);
-                            const half2 e02 = __hadd2(x0, x2), d02 = __hsub2(x0, x2);
-                            const half2 e13 = __hadd2(x1, x3), d13 = __hsub2(x1, x3);
-                            // i * d13 = (-d13.im, d13.re)
-                            const half2 id13 = __hmul2(__lowhigh2highlow(d13),
-                                                       __halves2half2(__float2half(-1.f), __float2half(1.f)));
-                            Z[i][0] = __hsub2(e02, e13);                  // x0 - x1 + x2 - x3
-                            Z[i][R > 1 ? 1 : 0] = __hadd2(d02, id13);     // x0 + i x1 - x2 - i x3
-                            Z[i][R > 2 ? 2 : 0] = __hadd2(e02, e13);      // x0 + x1 + x2 + x3
-                            Z[i][R > 3 ? 3 : 0] = __hsub2(d02, id13);     // x0 - i x1 - x2 + i x3
-                        }
-                    }
-#pragma unroll
-                    for (int kk = 0; kk < R; kk++) {
-                        uint4 vr, vi;
-                        uint32_t* pr = &vr.x;
-                        uint32_t* pi = &vi.x;
-#pragma unroll
-                        for (int i = 0; i < 4; i++) {
-                            const uint32_t lo = h2u(Z[2 * i][kk]), hi = h2u(Z[2 * i + 1][kk]);
-                            pr[i] = __byte_perm(lo, hi, 0x5410);  // (re_a, re_a+1)
-                            pi[i] = __byte_perm(lo, hi, 0x7632);  // (im_a, im_a+1)
-                        }
-                        const uint32_t r = kk * spectra + s;
-                        const uint32_t off = cm_off(r, grp, KA);
-                        *reinterpret_cast<uint4*>(stage + (p * 2 + 0) * blkA + off) = vr;
-                        *reinterpret_cast<uint4*>(stage + (p * 2 + 1) * blkA + off) = vi;
-                    }
-                }
+        uint32_t rs = 0, rph = 0, as = 0, aph = 0;
+        bool ok = true;
+        for (uint64_t L = L0; L < L1 && ok; L++) {
+            if (!mbar_wait(&r_full[rs], rph, abort, kWaitBudget)) { record_abort(abort, 11); break; }
+            const uint8_t* raw = r_smem + (size_t)rs * g.raw_bytes;
+            for (int p = 0; p < 2; p++) {
+                if (!mbar_wait(&a_empty[as], aph ^ 1, abort, kWaitBudget)) { record_abort(abort, 8); ok = false; break; }
+                build_operand<R>(raw, a_smem + (size_t)as * op_bytes, g.A, KA, p, ct);
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&a_full[as]);
+                if (++as == AS) { as = 0; aph ^= 1; }
             }
-            fence_proxy_async_smem();
+            if (!ok) break;
             __syncwarp();
-            if (lane == 0) mbar_arrive(&a_full[st]);
-            if (++st == S) { st = 0; aph ^= 1; }
+            if (lane == 0) mbar_arrive(&r_empty[rs]);
+            if (++rs == RS) { rs = 0; rph ^= 1; }
         }
     }
 
@@ -366,14 +489,19 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g) {
 }
 
 // ---- phasor image ------------------------------------------------------------
-// plan[chunk][f][p][h][blk][core-matrix layout of NB x KA fp16],
-// blk 0 = -Wi, 1 = Wr, 2 = Wi; h 0 = hi = rn(w), h 1 = lo = rn(w - hi).
+// plan[chunk][f][p][h] in the 128-byte-swizzled K-major layout, h 0 = hi = rn(w),
+// h 1 = lo = rn(w - hi):
+//   KA = 64: three blocks of NB rows x 64 K: [-Wi | Wr | Wi]
+//   KA = 32: one block of 2 NB rows x 64 K: rows b = [Wr | -Wi], rows NB + b = [Wi | Wr]
+__device__ __forceinline__ void put_half(uint8_t* blk, uint32_t row, uint32_t k, __half v) {
+    *reinterpret_cast<__half*>(blk + sw128_off(row, (k >> 3) & 7u) + (k & 7u) * 2u) = v;
+}
+
 __global__ void __launch_bounds__(256) tc_prepare_kernel(const float2* __restrict__ ph, uint8_t* __restrict__ plan,
                                                          uint32_t B, uint32_t A, uint32_t F, uint32_t NB,
-                                                         uint32_t KA, uint32_t nchunks) {
+                                                         uint32_t KA, uint32_t nchunks, uint32_t img_bytes) {
     const uint64_t n = (uint64_t)nchunks * F * 2 * NB * KA;
-    const uint32_t blk = NB * KA * 2;
-    const uint64_t img = 12ull * blk;
+    const uint32_t ph_bytes = (KA == 64 ? 3u : 2u) * NB * 128u;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t a = (uint32_t)(i % KA);
@@ -386,28 +514,33 @@ __global__ void __launch_bounds__(256) tc_prepare_kernel(const float2* __restric
         const uint32_t c = (uint32_t)(r / F);
         const uint32_t b = c * kMaxNB + nb;
         float wr = 0.f, wi = 0.f;
-        if (a < A && b < B && nb < NB) {
+        if (a < A && b < B) {
             const float2 w = ph[((uint64_t)(b * (uint64_t)A + a) * F + f) * 2 + p];
             wr = w.x;
             wi = w.y;
         }
         const __half rh = __float2half_rn(wr), ih = __float2half_rn(wi);
         const __half rl = __float2half_rn(wr - __half2float(rh)), il = __float2half_rn(wi - __half2float(ih));
-        uint8_t* base = plan + ((uint64_t)c * F + f) * img;
-        const uint32_t off = (nb >> 3) * (16u * KA) + (a >> 3) * 128u + (nb & 7u) * 16u + (a & 7u) * 2u;
-        __half* hb = reinterpret_cast<__half*>(base + (p * 2 + 0) * 3 * blk + off);
-        __half* lb = reinterpret_cast<__half*>(base + (p * 2 + 1) * 3 * blk + off);
-        hb[0] = __hneg(ih);
-        hb[blk / 2] = rh;
-        hb[blk] = ih;
-        lb[0] = __hneg(il);
-        lb[blk / 2] = rl;
-        lb[blk] = il;
+        uint8_t* base = plan + ((uint64_t)c * F + f) * img_bytes + (uint64_t)p * 2 * ph_bytes;
+        for (int h = 0; h < 2; h++) {
+            uint8_t* blk = base + h * ph_bytes;
+            const __half re = h ? rl : rh, im = h ? il : ih;
+            if (KA == 64) {
+                put_half(blk, nb, a, __hneg(im));                 // block 0: -Wi
+                put_half(blk + NB * 128u, nb, a, re);             // block 1:  Wr
+                put_half(blk + 2u * NB * 128u, nb, a, im);        // block 2:  Wi
+            } else {
+                put_half(blk, nb, a, re);                         // row b,      K < 32:  Wr
+                put_half(blk, nb, 32u + a, __hneg(im));           // row b,      K >= 32: -Wi
+                put_half(blk, NB + nb, a, im);                    // row NB + b, K < 32:  Wi
+                put_half(blk, NB + nb, 32u + a, re);              // row NB + b, K >= 32: Wr
+            }
+        }
     }
 }
 
 struct TcShape {
-    uint32_t NB, KA, nchunks, img_bytes, stages;
+    uint32_t NB, KA, nchunks, img_bytes, raw_bytes, a_stages, r_stages;
     size_t smem;
 };
 
@@ -415,21 +548,47 @@ bool tc_shape(uint64_t B, uint64_t A, TcShape& s) {
     if (A == 0 || A > kMaxKA || B == 0) return false;
     const uint64_t bc = B < (uint64_t)kMaxNB ? B : (uint64_t)kMaxNB;
     s.NB = (uint32_t)((bc + 15) / 16 * 16);
-    s.KA = (uint32_t)((A + 15) / 16 * 16);
+    s.KA = A <= 32 ? 32u : 64u;
     s.nchunks = (uint32_t)((B + kMaxNB - 1) / kMaxNB);
-    s.img_bytes = 12u * s.NB * s.KA * 2u;
-    const size_t stage = 4ull * kM * s.KA * 2;
-    const size_t fixed = s.img_bytes + 256;  // barriers, TMEM slot, abort flag
+    s.img_bytes = (s.KA == 64 ? 1536u : 1024u) * s.NB;
+    s.raw_bytes = (uint32_t)A * 512u;
+    const size_t op = (2ull * s.KA / 64) * 16384;   // one polarisation's operand
+    const size_t fixed = s.img_bytes + 256 + 1024;  // barriers, TMEM slot, abort flag, alignment slack
     const size_t limit = 227 * 1024;
-    size_t st = (limit - fixed) / stage;
-    if (st > 4) st = 4;
-    if (st < 2) return false;
-    s.stages = (uint32_t)st;
-    s.smem = fixed + st * stage;
+    uint32_t as = 4, rs = 6;
+    while (fixed + as * op + rs * (size_t)s.raw_bytes > limit) {
+        if (rs > 2 && rs >= as) rs--;
+        else if (as > 2) as--;
+        else if (rs > 1) rs--;
+        else return false;
+    }
+    s.a_stages = as;
+    s.r_stages = rs;
+    s.smem = fixed + as * op + rs * (size_t)s.raw_bytes;
     return true;
 }
 
-int g_tc_sms = 0;
+using TcKernel = void (*)(const TcArgs);
+
+template <int R>
+TcKernel pick_logi(uint32_t logi) {
+    switch (logi) {
+        case 0: return bf_tc_kernel<R, 0>;
+        case 1: return bf_tc_kernel<R, 1>;
+        case 2: return bf_tc_kernel<R, 2>;
+        case 3: return bf_tc_kernel<R, 3>;
+        case 4: return bf_tc_kernel<R, 4>;
+        default: return bf_tc_kernel<R, 5>;
+    }
+}
+
+TcKernel pick_kernel(uint64_t rate, uint64_t integration) {
+    uint32_t logi = 0;
+    while ((1ull << logi) < integration) logi++;
+    if (rate == 1) return pick_logi<1>(logi);
+    if (rate == 2) return pick_logi<2>(logi);
+    return pick_logi<4>(logi);
+}
 
 }  // namespace
 }  // namespace bb
@@ -455,7 +614,7 @@ extern "C" int blade_beamform_tc_prepare(const void* phasors, void* plan, uint64
     const uint64_t n = (uint64_t)s.nchunks * F * 2 * s.NB * s.KA;
     tc_prepare_kernel<<<grid_for(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         static_cast<const float2*>(phasors), static_cast<uint8_t*>(plan), (uint32_t)B, (uint32_t)A, (uint32_t)F,
-        s.NB, s.KA, s.nchunks);
+        s.NB, s.KA, s.nchunks, s.img_bytes);
     return check_launch("blade_beamform_tc_prepare");
 }
 
@@ -466,7 +625,7 @@ extern "C" int blade_beamform_detect_tc_supported(uint64_t B, uint64_t A, uint64
     if (rate != 1 && rate != 2 && rate != 4) return 0;
     if (integration == 0 || integration > 32 || (integration & (integration - 1)) != 0) return 0;
     if (T == 0 || T % kM != 0 || F == 0) return 0;
-    if (F > 0xffffffffull / (T / kM) || T >= (1ull << 31)) return 0;
+    if (F > 0xffffffffull / (T / kM) || T >= (1ull << 31) || (uint64_t)A * F * T >= (1ull << 40)) return 0;
     return 1;
 }
 
@@ -485,10 +644,8 @@ extern "C" int blade_beamform_detect_tc(const void* in, const void* plan, void* 
     TcShape s;
     tc_shape(B, A, s);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const void* fn = rate == 1 ? reinterpret_cast<const void*>(bf_tc_kernel<1>)
-                     : rate == 2 ? reinterpret_cast<const void*>(bf_tc_kernel<2>)
-                                 : reinterpret_cast<const void*>(bf_tc_kernel<4>);
-    if (int rc = ensure_smem(fn, s.smem)) return rc;
+    const TcKernel fn = pick_kernel(rate, integration);
+    if (int rc = ensure_smem(reinterpret_cast<const void*>(fn), s.smem)) return rc;
     const uint32_t U = (uint32_t)(T / (rate * integration));
     for (uint32_t c = 0; c < s.nchunks; c++) {
         TcArgs g;
@@ -501,21 +658,19 @@ extern "C" int blade_beamform_detect_tc(const void* in, const void* plan, void* 
         const uint64_t rem = B - (uint64_t)c * kMaxNB;
         g.beams = (uint32_t)(rem < (uint64_t)kMaxNB ? rem : kMaxNB);
         g.U = U;
-        g.integ = (uint32_t)integration;
         g.NB = s.NB;
         g.KA = s.KA;
-        g.stages = s.stages;
+        g.a_stages = s.a_stages;
+        g.r_stages = s.r_stages;
         g.img_bytes = s.img_bytes;
+        g.raw_bytes = s.raw_bytes;
         g.tiles_per_ch = (uint32_t)(T / kM);
         g.total_tiles = (uint64_t)F * (T / kM);
         uint64_t grid = (uint64_t)sm_count();
         if (grid > g.total_tiles) grid = g.total_tiles;
-        if (rate == 1) bf_tc_kernel<1><<<(unsigned)grid, kThreads, s.smem, st>>>(g);
-        else if (rate == 2) bf_tc_kernel<2><<<(unsigned)grid, kThreads, s.smem, st>>>(g);
-        else bf_tc_kernel<4><<<(unsigned)grid, kThreads, s.smem, st>>>(g);
+        fn<<<(unsigned)grid, kThreads, s.smem, st>>>(g);
         if (int rc = check_launch("blade_beamform_detect_tc")) return rc;
     }
-    (void)g_tc_sms;
     return BLADE_SUCCESS;
 }
 

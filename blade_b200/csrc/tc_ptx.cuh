@@ -139,6 +139,26 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
     return d;                // base offset 0, layout type 0 (no swizzle)
 }
 
+// Shared-memory matrix descriptor, K-major with the 128-byte swizzle: rows of
+// 128 bytes (64 FP16 along K), 8-row atoms of 1024 bytes (SBO = 1024), 16-byte
+// chunk c of row r stored at chunk position c ^ (r % 8).  The atom base must be
+// 1024-byte aligned; a K step of 16 elements advances the start address by 32 bytes.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;            // LBO (unused for swizzled K-major) = 16 bytes
+    d |= (uint64_t)(1024 >> 4) << 32;  // SBO = 1024 bytes between 8-row atoms
+    d |= (uint64_t)1 << 46;            // descriptor version for sm_100
+    d |= (uint64_t)2 << 61;            // layout type: SWIZZLE_128B
+    return d;
+}
+
+// Byte offset of the 16-byte chunk `chunk` (0..7) of row `row` inside a
+// 128-byte-swizzled block whose base is 1024-byte aligned.
+__host__ __device__ __forceinline__ uint32_t sw128_off(uint32_t row, uint32_t chunk) {
+    return (row >> 3) * 1024u + (row & 7u) * 128u + ((chunk ^ (row & 7u)) << 4);
+}
+
 // Instruction descriptor for kind::f16: A = B = F16, D = F32, both K-major.
 __host__ __device__ constexpr uint32_t idesc_f16(uint32_t M, uint32_t N) {
     return (1u << 4)               // D format F32

@@ -1,0 +1,70 @@
+"""Runs one hot-path kernel on one workload a few times, for profilers.
+
+    python -m blade_b200.profile_case --workload ata-production --path tc --launches 4
+
+Workloads: ata-small (A=20 F=96 T=256 B=8 rate 1 I=4), ata-production
+(A=28 F=192 T=8192 B=16 rate 4 I=4), dense-64x64 (A=64 F=256 T=8192 B=64 rate 1
+I=8).  Paths: tc (phasor split + tensor-core chain), f32 (fused FP32 chain),
+modules (Cast -> Beamformer -> Channelizer -> Detector, one launch each).
+Inputs are seeded synthetic CI8 voltages and phasors, created on the device.
+"""
+
+from __future__ import annotations
+
+import argparse
+
+import torch
+
+from . import _lib
+from .synthetic import DF_HZ, F0_HZ
+
+WORKLOADS = {
+    "ata-small": dict(A=20, F=96, T=256, B=8, R=1, I=4),
+    "ata-production": dict(A=28, F=192, T=8192, B=16, R=4, I=4),
+    "dense-64x64": dict(A=64, F=256, T=8192, B=64, R=1, I=8),
+}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="ata-production", choices=sorted(WORKLOADS))
+    ap.add_argument("--path", default="tc", choices=["tc", "f32", "modules"])
+    ap.add_argument("--launches", type=int, default=4)
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    A, F, T, B, R, I, P = w["A"], w["F"], w["T"], w["B"], w["R"], w["I"], 2
+    lib = _lib.load()
+    s = torch.cuda.current_stream().cuda_stream
+    g = torch.Generator(device="cuda").manual_seed(7)
+    x = (torch.randn((A, F, T, P, 2), generator=g, device="cuda") * 8).round_().clamp_(-127, 127).to(torch.int8)
+    tau = (torch.rand((B, A), generator=g, device="cuda", dtype=torch.float64) * 2 - 1) * 5e-6
+    ph = torch.empty((B, A, F, 1, P), dtype=torch.complex64, device="cuda")
+    _lib.call("blade_phasor_from_delays", tau.data_ptr(), None, ph.data_ptr(), B, A, F, P, F0_HZ, DF_HZ, 0.0, 0, s)
+    out = torch.empty((B, F * R, T // (R * I), 1), dtype=torch.float32, device="cuda")
+    if args.path == "tc":
+        plan = torch.empty(int(lib.blade_beamform_tc_plan_size(B, A, F, P)), dtype=torch.uint8, device="cuda")
+        for _ in range(args.launches):
+            _lib.call("blade_beamform_tc_prepare", ph.data_ptr(), plan.data_ptr(), B, A, F, P, s)
+            _lib.call("blade_beamform_detect_tc", x.data_ptr(), plan.data_ptr(), out.data_ptr(), B, A, F, T, P, R, I, s)
+    elif args.path == "f32":
+        for _ in range(args.launches):
+            _lib.call("blade_beamform_detect_f32", _lib.CI8, x.data_ptr(), ph.data_ptr(), out.data_ptr(), B, A, F, T,
+                      P, R, I, s)
+    else:
+        xf = torch.empty((A, F, T, P), dtype=torch.complex64, device="cuda")
+        y = torch.empty((B, F, T, P), dtype=torch.complex64, device="cuda")
+        yc = torch.empty((B, F * R, T // R, P), dtype=torch.complex64, device="cuda")
+        for _ in range(args.launches):
+            _lib.call("blade_cast", _lib.CI8, _lib.CF32, x.data_ptr(), xf.data_ptr(), A * F * T * P, s)
+            _lib.call("blade_beamform_f32", xf.data_ptr(), ph.data_ptr(), y.data_ptr(), B, A, F, T, P, 0, 0, s)
+            if R > 1:
+                _lib.call("blade_channelize", y.data_ptr(), yc.data_ptr(), None, B, F, T, P, R, s)
+            else:
+                yc = y
+            _lib.call("blade_detect", yc.data_ptr(), out.data_ptr(), B, F * R, T // R, P, I, 1, s)
+    torch.cuda.synchronize()
+    print(f"{args.workload} {args.path}: {args.launches} launches ok")
+
+
+if __name__ == "__main__":
+    main()
