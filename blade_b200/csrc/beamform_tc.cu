@@ -40,6 +40,9 @@
 // and polarisation), two TMEM accumulator buffers, the phasor image.  Every wait
 // is bounded (clock budget plus a shared abort flag); on expiry the kernel records
 // a status word, drains its own MMAs and bulk copies, frees TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <mutex>
 
 #include "common.cuh"
@@ -68,7 +71,7 @@ struct TcArgs {
     const uint8_t* plan;  // phasor images, one per channel, img_bytes each
     float* out;           // [beams, F*R, U]
     uint32_t A, F, T, beams, U;
-    uint32_t NB, KA, a_stages, r_stages;
+    uint32_t NB, KA, a_stages, r_stages, stacked;
     uint32_t img_bytes, raw_bytes, tiles_per_ch;
     uint64_t total_tiles;
 };
@@ -252,8 +255,44 @@ __device__ __forceinline__ int window_reduce(float (&v)[16], uint32_t lane, uint
     return 16 >> RS;
 }
 
+// ---- MMA issue ----------------------------------------------------------------
+// Descriptors are built once per stage and stepped by adding 16-byte units to the
+// start-address field, so each tcgen05.mma costs a handful of integer adds.
+// A operand k-step j: column block j / 4 (16 KB each), 32 bytes per step in a row.
+__device__ __forceinline__ uint64_t a_step(uint64_t ad, int j) {
+    return ad + (uint64_t)((((j >> 2) * 16384) + (j & 3) * 32) >> 4);
+}
+
+// hi and lo stacked along N (4 NB rows per column block of the image): one MMA per k-step.
+template <int KSTEPS>
+__device__ __forceinline__ void issue_stacked(uint32_t d, uint64_t ad, uint64_t wd, uint32_t wblk16, uint32_t idesc) {
+#pragma unroll
+    for (int j = 0; j < KSTEPS; j++)
+        mma_f16(d, a_step(ad, j), wd + (uint64_t)((j >> 2) * wblk16 + (j & 3) * 2), idesc, j > 0 ? 1u : 0u);
+}
+
+// KA = 64, hi and lo as separate MMAs: the Xr steps read blocks [Wr | Wi], the Xi
+// steps [-Wi | Wr] of the [-Wi | Wr | Wi] image (nb16 = one block, 16-byte units).
+__device__ __forceinline__ void issue_ka64(uint32_t d, uint64_t ad, uint64_t wd, uint32_t nb16, uint32_t idesc) {
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+            mma_f16(d, a_step(ad, j), wd + (uint64_t)(h * 3 * nb16 + (j < 4 ? nb16 : 0) + (j & 3) * 2), idesc,
+                    (h | j) ? 1u : 0u);
+}
+
+// KA = 32, hi and lo as separate MMAs over one block of 2 NB rows per (p, h).
+__device__ __forceinline__ void issue_ka32(uint32_t d, uint64_t ad, uint64_t wd, uint32_t nb16, uint32_t idesc) {
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            mma_f16(d, a_step(ad, j), wd + (uint64_t)(h * 2 * nb16 + j * 2), idesc, (h | j) ? 1u : 0u);
+}
+
 template <int R, int LOGI>
-__global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g) {
+__global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, const __grid_constant__ CUtensorMap tmap) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // Swizzled operands need 1024-byte aligned atoms: align the working base.
     uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -277,7 +316,11 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g) {
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     volatile int never = 0;  // abort flag that is never raised (drain waits)
-    const uint32_t tmem_cols = (8 * NB <= 32) ? 32 : (8 * NB <= 64) ? 64 : (8 * NB <= 128) ? 128 : (8 * NB <= 256) ? 256 : 512;
+    // Accumulator columns per polarisation: [re | im] (2 NB), or with hi/lo stacked
+    // along N [hi re | hi im | lo re | lo im] (4 NB); two tiles in flight.
+    const uint32_t d_cols = (g.stacked ? 4u : 2u) * NB;
+    const uint32_t need_cols = 4 * d_cols;
+    const uint32_t tmem_cols = need_cols <= 32 ? 32 : need_cols <= 64 ? 64 : need_cols <= 128 ? 128 : need_cols <= 256 ? 256 : 512;
 
     if (threadIdx.x == 0) {
         for (uint32_t i = 0; i < AS; i++) {
@@ -316,12 +359,15 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g) {
     if (warp == 0) {
         // ---------------- MMA issuer ----------------
         if (lane == 0 && L0 < L1) {
-            const uint32_t idesc = idesc_f16(kM, 2 * NB);
-            const uint32_t w_base = smem_u32(w_smem), a_base = smem_u32(a_smem);
-            const uint32_t ksteps = 2 * KA / 16;
-            // Phasor image per (p, h): KA = 64 -> blocks [-Wi | Wr | Wi] of NB rows;
-            // KA = 32 -> one block of 2 NB rows ([Wr | -Wi] over [Wi | Wr]).
-            const uint32_t ph_bytes = (KA == 64 ? 3u : 2u) * NB * 128u;
+            const uint32_t idesc = idesc_f16(kM, d_cols);
+            const uint64_t w_desc = smem_desc_sw128(smem_u32(w_smem));
+            const uint64_t a_desc = smem_desc_sw128(smem_u32(a_smem));
+            const uint32_t op16 = op_bytes >> 4;   // operand stage stride, 16-byte units
+            const uint32_t nb16 = NB * 8;          // NB rows x 128 bytes, 16-byte units
+            // Phasor image stride per polarisation, 16-byte units:
+            //   stacked: (2 KA / 64) column blocks of 4 NB rows;
+            //   KA = 64: two (hi, lo) x three NB-row blocks; KA = 32: two x one 2 NB-row block.
+            const uint32_t wpol16 = g.stacked ? (2 * KA / 64) * 4 * nb16 : (KA == 64 ? 6 * nb16 : 4 * nb16);
             uint32_t as = 0, aph = 0, db = 0, dph = 0, wph = 0;
             bool ok = true;
             for (uint64_t L = L0; L < L1 && ok; L++) {
@@ -333,19 +379,16 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g) {
                 for (uint32_t p = 0; p < 2; p++) {
                     if (!mbar_wait(&a_full[as], aph, abort, kWaitBudget)) { record_abort(abort, 2); ok = false; break; }
                     tc_fence_after();
-                    const uint32_t a_stage = a_base + as * op_bytes;
-                    const uint32_t d = tmem + db * (4 * NB) + p * (2 * NB);
-                    uint32_t acc = 0;
-                    for (uint32_t h = 0; h < 2; h++) {
-                        const uint32_t wph_base = w_base + (p * 2 + h) * ph_bytes;
-                        for (uint32_t j = 0; j < ksteps; j++) {
-                            const uint32_t aaddr = a_stage + (j >> 2) * 16384u + (j & 3u) * 32u;
-                            uint32_t baddr;
-                            if (KA == 64) baddr = wph_base + (j < 4 ? NB * 128u : 0u) + (j & 3u) * 32u;
-                            else baddr = wph_base + j * 32u;
-                            mma_f16(d, smem_desc_sw128(aaddr), smem_desc_sw128(baddr), idesc, acc);
-                            acc = 1;
-                        }
+                    const uint64_t ad = a_desc + (uint64_t)(as * op16);
+                    const uint64_t wd = w_desc + (uint64_t)(p * wpol16);
+                    const uint32_t d = tmem + db * (2 * d_cols) + p * d_cols;
+                    if (g.stacked) {
+                        if (KA == 64) issue_stacked<8>(d, ad, wd, 4 * nb16, idesc);
+                        else issue_stacked<4>(d, ad, wd, 4 * nb16, idesc);
+                    } else if (KA == 64) {
+                        issue_ka64(d, ad, wd, nb16, idesc);
+                    } else {
+                        issue_ka32(d, ad, wd, nb16, idesc);
                     }
                     mma_commit(&a_empty[as]);
                     if (++as == AS) { as = 0; aph ^= 1; }
@@ -389,15 +432,17 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g) {
                 }
                 if (lane == 0) {
                     ok = mbar_wait(&r_empty[rs], rph ^ 1, abort, kWaitBudget);
-                    if (ok) mbar_arrive_expect_tx(&r_full[rs], g.A * 512u);
-                    else record_abort(abort, 9);
+                    if (ok) {
+                        // One tensor load per tile: 128 samples x 1 channel x A antennas,
+                        // landing antenna-major (512 bytes per antenna) in the raw stage.
+                        mbar_arrive_expect_tx(&r_full[rs], g.A * 512u);
+                        tma_load_3d(r_smem + (size_t)rs * g.raw_bytes, &tmap, (int)(tt * kM), (int)f, 0, &r_full[rs]);
+                    } else {
+                        record_abort(abort, 9);
+                    }
                 }
                 ok = __shfl_sync(0xffffffffu, ok, 0);
                 if (!ok) break;
-                uint8_t* dst = r_smem + (size_t)rs * g.raw_bytes;
-                const uint8_t* src = g.in + ((uint64_t)f * g.T + (uint64_t)tt * kM) * 4;
-                for (uint32_t a = lane; a < g.A; a += 32)
-                    bulk_g2s(dst + a * 512, src + (uint64_t)a * g.F * g.T * 4, 512, &r_full[rs]);
                 issued_mask |= 1u << rs;
                 issued_par = (issued_par & ~(1u << rs)) | (rph << rs);
                 if (++rs == RS) { rs = 0; rph ^= 1; }
@@ -425,22 +470,44 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g) {
             tc_fence_after();
             const uint32_t f = (uint32_t)(L / tpc), tt = (uint32_t)(L % tpc);
             const uint32_t u = (tt * rows_per_k + s_local) / I;
-            const uint32_t lane_addr = tmem + ((32 * q) << 16) + db * (4 * NB);
+            const uint32_t lane_addr = tmem + ((32 * q) << 16) + db * (2 * d_cols);
             float* obase = g.out + ((uint64_t)f * R + k) * g.U + u;
             const uint64_t bstride = (uint64_t)g.F * R * g.U;
             for (uint32_t bc = 0; bc < NB; bc += 16) {
-                uint32_t r0[16], i0[16], r1[16], i1[16];
-                tmem_ld16(lane_addr + bc, r0);
-                tmem_ld16(lane_addr + NB + bc, i0);
-                tmem_ld16(lane_addr + 2 * NB + bc, r1);
-                tmem_ld16(lane_addr + 3 * NB + bc, i1);
-                tmem_ld_wait();
                 float pw[16];
+                if (g.stacked) {
+                    // per polarisation: (hi + lo) re, (hi + lo) im
 #pragma unroll
-                for (int j = 0; j < 16; j++) {
-                    const float a0 = __uint_as_float(r0[j]), b0 = __uint_as_float(i0[j]);
-                    const float a1 = __uint_as_float(r1[j]), b1 = __uint_as_float(i1[j]);
-                    pw[j] = fmaf(a0, a0, fmaf(b0, b0, fmaf(a1, a1, b1 * b1)));
+                    for (int j = 0; j < 16; j++) pw[j] = 0.f;
+#pragma unroll
+                    for (uint32_t p = 0; p < 2; p++) {
+                        uint32_t hr[16], hi[16], lr[16], li[16];
+                        const uint32_t pa = lane_addr + p * d_cols + bc;
+                        tmem_ld16(pa, hr);
+                        tmem_ld16(pa + NB, hi);
+                        tmem_ld16(pa + 2 * NB, lr);
+                        tmem_ld16(pa + 3 * NB, li);
+                        tmem_ld_wait();
+#pragma unroll
+                        for (int j = 0; j < 16; j++) {
+                            const float a = __uint_as_float(hr[j]) + __uint_as_float(lr[j]);
+                            const float b = __uint_as_float(hi[j]) + __uint_as_float(li[j]);
+                            pw[j] = fmaf(a, a, fmaf(b, b, pw[j]));
+                        }
+                    }
+                } else {
+                    uint32_t r0[16], i0[16], r1[16], i1[16];
+                    tmem_ld16(lane_addr + bc, r0);
+                    tmem_ld16(lane_addr + NB + bc, i0);
+                    tmem_ld16(lane_addr + 2 * NB + bc, r1);
+                    tmem_ld16(lane_addr + 3 * NB + bc, i1);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int j = 0; j < 16; j++) {
+                        const float a0 = __uint_as_float(r0[j]), b0 = __uint_as_float(i0[j]);
+                        const float a1 = __uint_as_float(r1[j]), b1 = __uint_as_float(i1[j]);
+                        pw[j] = fmaf(a0, a0, fmaf(b0, b0, fmaf(a1, a1, b1 * b1)));
+                    }
                 }
                 uint32_t first;
                 const int cnt = window_reduce<LOGI>(pw, lane, &first);
@@ -489,19 +556,28 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g) {
 }
 
 // ---- phasor image ------------------------------------------------------------
-// plan[chunk][f][p][h] in the 128-byte-swizzled K-major layout, h 0 = hi = rn(w),
-// h 1 = lo = rn(w - hi):
-//   KA = 64: three blocks of NB rows x 64 K: [-Wi | Wr | Wi]
-//   KA = 32: one block of 2 NB rows x 64 K: rows b = [Wr | -Wi], rows NB + b = [Wi | Wr]
+// plan[chunk][f][p] in the 128-byte-swizzled K-major layout (K = 2 KA: Xr part
+// then Xi part), h 0 = hi = rn(w), h 1 = lo = rn(w - hi):
+//   stacked (NB <= 32): per p, (2 KA / 64) column blocks of 4 NB rows
+//            [hi: b -> (Wr | -Wi), NB + b -> (Wi | Wr) ; lo: the same],
+//   KA = 64, NB > 32: per (p, h) three blocks of NB rows x 64 K: [-Wi | Wr | Wi],
+//   KA = 32, NB > 32: per (p, h) one block of 2 NB rows: b -> [Wr | -Wi], NB + b -> [Wi | Wr].
 __device__ __forceinline__ void put_half(uint8_t* blk, uint32_t row, uint32_t k, __half v) {
     *reinterpret_cast<__half*>(blk + sw128_off(row, (k >> 3) & 7u) + (k & 7u) * 2u) = v;
 }
 
+// K index k_total over several 64-wide column blocks of `rows` rows each.
+__device__ __forceinline__ void put_half_k(uint8_t* base, uint32_t rows, uint32_t row, uint32_t k_total, __half v) {
+    put_half(base + (k_total >> 6) * rows * 128u, row, k_total & 63u, v);
+}
+
 __global__ void __launch_bounds__(256) tc_prepare_kernel(const float2* __restrict__ ph, uint8_t* __restrict__ plan,
                                                          uint32_t B, uint32_t A, uint32_t F, uint32_t NB,
-                                                         uint32_t KA, uint32_t nchunks, uint32_t img_bytes) {
+                                                         uint32_t KA, uint32_t nchunks, uint32_t img_bytes,
+                                                         uint32_t stacked) {
     const uint64_t n = (uint64_t)nchunks * F * 2 * NB * KA;
     const uint32_t ph_bytes = (KA == 64 ? 3u : 2u) * NB * 128u;
+    const uint32_t pol_stacked = (2 * KA / 64) * 4 * NB * 128u;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t a = (uint32_t)(i % KA);
@@ -521,6 +597,19 @@ __global__ void __launch_bounds__(256) tc_prepare_kernel(const float2* __restric
         }
         const __half rh = __float2half_rn(wr), ih = __float2half_rn(wi);
         const __half rl = __float2half_rn(wr - __half2float(rh)), il = __float2half_rn(wi - __half2float(ih));
+        if (stacked) {
+            uint8_t* base = plan + ((uint64_t)c * F + f) * img_bytes + (uint64_t)p * pol_stacked;
+            const uint32_t rows = 4 * NB;
+            for (uint32_t h = 0; h < 2; h++) {
+                const __half re = h ? rl : rh, im = h ? il : ih;
+                const uint32_t rr = h * 2 * NB + nb, ri = h * 2 * NB + NB + nb;
+                put_half_k(base, rows, rr, a, re);                // Re-output row, Xr part:  Wr
+                put_half_k(base, rows, rr, KA + a, __hneg(im));   // Re-output row, Xi part: -Wi
+                put_half_k(base, rows, ri, a, im);                // Im-output row, Xr part:  Wi
+                put_half_k(base, rows, ri, KA + a, re);           // Im-output row, Xi part:  Wr
+            }
+            continue;
+        }
         uint8_t* base = plan + ((uint64_t)c * F + f) * img_bytes + (uint64_t)p * 2 * ph_bytes;
         for (int h = 0; h < 2; h++) {
             uint8_t* blk = base + h * ph_bytes;
@@ -540,7 +629,7 @@ __global__ void __launch_bounds__(256) tc_prepare_kernel(const float2* __restric
 }
 
 struct TcShape {
-    uint32_t NB, KA, nchunks, img_bytes, raw_bytes, a_stages, r_stages;
+    uint32_t NB, KA, nchunks, img_bytes, raw_bytes, a_stages, r_stages, stacked;
     size_t smem;
 };
 
@@ -550,7 +639,10 @@ bool tc_shape(uint64_t B, uint64_t A, TcShape& s) {
     s.NB = (uint32_t)((bc + 15) / 16 * 16);
     s.KA = A <= 32 ? 32u : 64u;
     s.nchunks = (uint32_t)((B + kMaxNB - 1) / kMaxNB);
-    s.img_bytes = (s.KA == 64 ? 1536u : 1024u) * s.NB;
+    // hi/lo stacked along N (one MMA per k-step, N = 4 NB <= 128) whenever the
+    // doubled accumulators still fit twice in tensor memory.
+    s.stacked = s.NB <= 32 ? 1u : 0u;
+    s.img_bytes = s.stacked ? (2 * s.KA / 64) * 1024u * s.NB : (s.KA == 64 ? 1536u : 1024u) * s.NB;
     s.raw_bytes = (uint32_t)A * 512u;
     const size_t op = (2ull * s.KA / 64) * 16384;   // one polarisation's operand
     const size_t fixed = s.img_bytes + 256 + 1024;  // barriers, TMEM slot, abort flag, alignment slack
@@ -568,7 +660,35 @@ bool tc_shape(uint64_t B, uint64_t A, TcShape& s) {
     return true;
 }
 
-using TcKernel = void (*)(const TcArgs);
+using TcKernel = void (*)(const TcArgs, const CUtensorMap);
+
+// Tensor map of the CI8 voltages seen as uint32 samples [A][F][T] (one 4-byte
+// word = both polarisations of one sample); box = 128 samples x 1 channel x A.
+int encode_voltage_map(CUtensorMap* tm, const void* in, uint64_t A, uint64_t F, uint64_t T) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static std::mutex mu;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!encode) {
+            cudaDriverEntryPointQueryResult q;
+            void* fn = nullptr;
+            if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) !=
+                    cudaSuccess ||
+                q != cudaDriverEntryPointSuccess || !fn)
+                return set_error(BLADE_CUDA_ERROR, "blade_beamform_detect_tc: cuTensorMapEncodeTiled unavailable");
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        }
+    }
+    const cuuint64_t dims[3] = {T, F, A};
+    const cuuint64_t strides[2] = {T * 4, F * T * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)kM, 1, (cuuint32_t)A};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, const_cast<void*>(in), dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(BLADE_CUDA_ERROR, "blade_beamform_detect_tc: tensor map encode (%d)", (int)r);
+    return BLADE_SUCCESS;
+}
 
 template <int R>
 TcKernel pick_logi(uint32_t logi) {
@@ -614,7 +734,7 @@ extern "C" int blade_beamform_tc_prepare(const void* phasors, void* plan, uint64
     const uint64_t n = (uint64_t)s.nchunks * F * 2 * s.NB * s.KA;
     tc_prepare_kernel<<<grid_for(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         static_cast<const float2*>(phasors), static_cast<uint8_t*>(plan), (uint32_t)B, (uint32_t)A, (uint32_t)F,
-        s.NB, s.KA, s.nchunks, s.img_bytes);
+        s.NB, s.KA, s.nchunks, s.img_bytes, s.stacked);
     return check_launch("blade_beamform_tc_prepare");
 }
 
@@ -647,6 +767,8 @@ extern "C" int blade_beamform_detect_tc(const void* in, const void* plan, void* 
     const TcKernel fn = pick_kernel(rate, integration);
     if (int rc = ensure_smem(reinterpret_cast<const void*>(fn), s.smem)) return rc;
     const uint32_t U = (uint32_t)(T / (rate * integration));
+    CUtensorMap tmap;
+    if (int rc = encode_voltage_map(&tmap, in, A, F, T)) return rc;
     for (uint32_t c = 0; c < s.nchunks; c++) {
         TcArgs g;
         g.in = static_cast<const uint8_t*>(in);
@@ -664,11 +786,12 @@ extern "C" int blade_beamform_detect_tc(const void* in, const void* plan, void* 
         g.r_stages = s.r_stages;
         g.img_bytes = s.img_bytes;
         g.raw_bytes = s.raw_bytes;
+        g.stacked = s.stacked;
         g.tiles_per_ch = (uint32_t)(T / kM);
         g.total_tiles = (uint64_t)F * (T / kM);
         uint64_t grid = (uint64_t)sm_count();
         if (grid > g.total_tiles) grid = g.total_tiles;
-        fn<<<(unsigned)grid, kThreads, s.smem, st>>>(g);
+        fn<<<(unsigned)grid, kThreads, s.smem, st>>>(g, tmap);
         if (int rc = check_launch("blade_beamform_detect_tc")) return rc;
     }
     return BLADE_SUCCESS;

@@ -219,7 +219,7 @@ BLADE_API int blade_device_status(uint32_t* status);
  * streaming callers whose device memory is sized once at start-up and whose
  * fixed-cadence loop cannot absorb the device synchronisation of an allocation.
  * Limit: blade_beamform_tc_plan_size(B, A, F, P) <= 8 MiB (e.g. A <= 32,
- * B <= 16 up to 682 channels); larger images are rejected with BLADE_ERROR.
+ * B <= 16 up to 512 channels); larger images are rejected with BLADE_ERROR.
  * The first call on each device looks up the array's device address (make that
  * first call before any stream capture).  All calls share the one array: calls
  * that overlap on the GPU (different streams, or different host threads) race;

@@ -83,8 +83,13 @@ def test_tc_support_query():
     assert lib.blade_beamform_detect_tc_supported(16, 28, 192, 8000, 2, 4, 4) == 0  # T % 128
     assert lib.blade_beamform_detect_tc_supported(16, 28, 192, 8192, 2, 8, 4) == 0  # rate
     assert lib.blade_beamform_detect_tc_supported(16, 28, 192, 8192, 2, 4, 3) == 0  # integration
-    assert lib.blade_beamform_tc_plan_size(64, 64, 256, 2) == 256 * 12 * 64 * 64 * 2
-    assert lib.blade_beamform_tc_plan_size(100, 20, 3, 2) == 2 * 3 * 12 * 64 * 32 * 2
+    # phasor image bytes per channel and 64-beam chunk: NB = beams rounded to 16,
+    # KA = 32 or 64; hi/lo stacked along N when NB <= 32: (2 KA / 64) * 1024 * NB,
+    # else 1536 * NB (KA = 64) or 1024 * NB (KA = 32).
+    assert lib.blade_beamform_tc_plan_size(64, 64, 256, 2) == 256 * 1536 * 64
+    assert lib.blade_beamform_tc_plan_size(100, 20, 3, 2) == 2 * 3 * 1024 * 64
+    assert lib.blade_beamform_tc_plan_size(16, 28, 192, 2) == 192 * 1024 * 16
+    assert lib.blade_beamform_tc_plan_size(32, 40, 5, 2) == 5 * 2 * 1024 * 32
 
 
 def test_channelize_workspace_size():
