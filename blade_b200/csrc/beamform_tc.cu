@@ -18,28 +18,34 @@
 //
 // GEMM mapping per (channel f, polarisation p): D[m, n] = sum_k A[m, k] B[n, k]
 // with m = one of 128 rows of a tile (R consecutive samples per spectrum,
-// row = k * (128/R) + spectrum), k = antenna (K = A padded to 16), and the complex
-// product embedded in reals with N = 2 NB (NB = beams padded to 16):
-//   D[:, 0:NB]   = Xr Wr - Xi Wi  (Re y),   D[:, NB:2NB] = Xr Wi + Xi Wr  (Im y)
-//   D = Xr . [Wr | Wi]^T + Xi . [-Wi | Wr]^T
-// The phasor image stores the three blocks [-Wi | Wr | Wi] per (p, hi/lo), so both
-// B operands are contiguous windows of it.  Operands use the K-major no-swizzle
-// core-matrix layout (8 rows x 16 bytes per 128-byte core matrix).
+// row = k * (128/R) + spectrum), k = [Xr of KA antennas | Xi of KA antennas]
+// (KA = 32 or 64, antennas zero-padded), and the complex product embedded in reals
+// (NB = beams of a 64-beam chunk padded to 16):
+//   Re y = Xr Wr - Xi Wi,   Im y = Xr Wi + Xi Wr
+// Three phasor-image layouts, all K-major with the 128-byte swizzle:
+//   NB <= 32 ("stacked"): rows [hi Re | hi Im | lo Re | lo Im] x NB, K = 2 KA, so
+//            one MMA per k-step with N = 4 NB gives both hi and lo products;
+//   KA = 64: blocks [-Wi | Wr | Wi] per (p, hi/lo); the Xr k-steps read the window
+//            [Wr | Wi], the Xi k-steps [-Wi | Wr] (N = 2 NB);
+//   KA = 32: one embedded block of 2 NB rows per (p, hi/lo), K = 2 KA.
+// Each 64-element K block of an operand is 128 rows x 128 bytes (16 KB).
 //
-// CTA organisation (persistent, one CTA per SM, 14 warps):
-//   warp 0      TMEM allocation; lane 0 issues tcgen05.mma and commits
+// CTA organisation (persistent, one CTA per SM, 15 warps):
+//   warp 0      TMEM allocation; lane 0 issues tcgen05.mma and commits (MMA
+//               issuer 0; warp 14 is issuer 1 when two issuers apply)
 //   warp 1      loader: the per-channel phasor image (one bulk copy) and the raw
-//               CI8 tiles (one 512-byte bulk copy per antenna row, all lanes),
-//               into a ring of raw stages several tiles ahead
+//               CI8 tiles (one 3-D TMA tensor load per tile: 128 samples x 1
+//               channel x A antennas) into a ring of raw stages
 //   warps 2-5   epilogue: tcgen05.ld of the accumulators, |.|^2 over both
 //               polarisations, window sums with lane shuffles, Stokes-I stores
 //   warps 6-13  operand build from the raw ring: DFT, exact int8 -> FP16
-//               conversion, stores in the UMMA core-matrix layout, one
-//               polarisation per operand stage
+//               conversion, swizzled stores; both polarisations of a tile in one
+//               pass when the operand ring holds at least two tiles
 // Pipelines (full/empty mbarrier pairs): raw stages, operand stages (one per tile
-// and polarisation), two TMEM accumulator buffers, the phasor image.  Every wait
-// is bounded (clock budget plus a shared abort flag); on expiry the kernel records
-// a status word, drains its own MMAs and bulk copies, frees TMEM and returns.
+// and polarisation), up to four TMEM accumulator buffers, the phasor image.  Every
+// wait is bounded (clock budget plus a shared abort flag) and sleeps on the
+// mbarrier rather than spinning; on expiry the kernel records a status word,
+// drains its own MMAs and copies, frees TMEM and returns.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -60,10 +66,14 @@ using namespace tc;
 
 constexpr int kM = 128;  // tile rows
 constexpr int kConvWarps = 8;
-constexpr int kEpiWarps = 4;
-constexpr int kThreads = (2 + kEpiWarps + kConvWarps) * 32;  // 448
+constexpr int kEpiWarps = 4;  // one or two per TMEM lane quarter
+constexpr int kEpiGroups = kEpiWarps / 4;  // warps per lane quarter, each a share of the beams
+constexpr int kWarps = 3 + kEpiWarps + kConvWarps;  // + MMA issuer 0, loader, MMA issuer 1
+constexpr int kThreads = kWarps * 32;               // 480
 constexpr int kMaxNB = 64;
 constexpr int kMaxKA = 64;
+constexpr int kMaxAcc = 4;   // TMEM accumulator buffers
+constexpr int kMaxStages = 8;  // operand stages and raw stages, each
 constexpr long long kWaitBudget = 4000000000ll;  // cycles (~2 s) before a wait gives up
 
 struct TcArgs {
@@ -73,6 +83,7 @@ struct TcArgs {
     uint32_t A, F, T, beams, U;
     uint32_t NB, KA, a_stages, r_stages, stacked;
     uint32_t img_bytes, raw_bytes, tiles_per_ch;
+    uint32_t raw_tiles, raw_row;  // tiles per raw stage (1, 2 or 4) and its antenna row stride (raw_tiles * 512)
     uint64_t total_tiles;
 };
 
@@ -93,6 +104,7 @@ __device__ __forceinline__ half2 sample_h2(uint32_t w, int p) {
 }
 
 __device__ __forceinline__ uint32_t h2u(half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
+__device__ __forceinline__ half2 u2h(uint32_t u) { return *reinterpret_cast<half2*>(&u); }
 
 // Address of K element k_total (a multiple of 4) of row `row` in one
 // polarisation's operand: Xr occupies k_total in [0, KA), Xi [KA, 2 KA); every
@@ -132,13 +144,14 @@ __device__ __forceinline__ void r1_chunks(const uint32_t (&w)[8], int p, uint4& 
     vi.w = cvt_pair(__byte_perm(w[6], w[7], sim));
 }
 
-// Builds the operand rows of polarisation p for one tile from the raw tile in
-// shared memory (antenna-major, 512 bytes = 128 samples x 4 bytes per antenna).
+// Builds the operand rows of polarisation p for one tile from the raw stage in
+// shared memory (antenna-major rows of rrow bytes; `raw` points at this tile's
+// 128 samples x 4 bytes in the first row).
 // Row = k * (128 / R) + spectrum.  Consecutive lanes take consecutive rows, so
 // every 16-byte store of a warp lands in a distinct bank group of the swizzle.
 template <int R>
-__device__ __forceinline__ void build_operand(const uint8_t* raw, uint8_t* op, uint32_t A, uint32_t KA, int p,
-                                              uint32_t ct) {
+__device__ __forceinline__ void build_operand(const uint8_t* raw, uint32_t rrow, uint8_t* op, uint32_t A, uint32_t KA,
+                                              int p, uint32_t ct) {
     constexpr uint32_t kStride = kConvWarps * 32;
     if constexpr (R == 1) {
         const uint32_t ntasks = kM * (KA / 8);
@@ -151,8 +164,8 @@ __device__ __forceinline__ void build_operand(const uint8_t* raw, uint8_t* op, u
 #pragma unroll
             for (int i = 0; i < 8; i++) {
                 const uint32_t a0 = g0 * 8 + i, a1 = g1 * 8 + i;
-                w0[i] = a0 < A ? *reinterpret_cast<const uint32_t*>(raw + a0 * 512 + s0 * 4) : 0u;
-                w1[i] = (has1 && a1 < A) ? *reinterpret_cast<const uint32_t*>(raw + a1 * 512 + s1 * 4) : 0u;
+                w0[i] = a0 < A ? *reinterpret_cast<const uint32_t*>(raw + a0 * rrow + s0 * 4) : 0u;
+                w1[i] = (has1 && a1 < A) ? *reinterpret_cast<const uint32_t*>(raw + a1 * rrow + s1 * 4) : 0u;
             }
             uint4 vr, vi;
             r1_chunks(w0, p, vr, vi);
@@ -172,7 +185,7 @@ __device__ __forceinline__ void build_operand(const uint8_t* raw, uint8_t* op, u
 #pragma unroll
             for (int i = 0; i < 8; i++) {
                 const uint32_t a = grp * 8 + i;
-                v[i] = a < A ? *reinterpret_cast<const uint2*>(raw + a * 512 + s * 8) : make_uint2(0u, 0u);
+                v[i] = a < A ? *reinterpret_cast<const uint2*>(raw + a * rrow + s * 8) : make_uint2(0u, 0u);
             }
             half2 Z0[8], Z1[8];
 #pragma unroll
@@ -207,7 +220,7 @@ __device__ __forceinline__ void build_operand(const uint8_t* raw, uint8_t* op, u
 #pragma unroll
             for (int i = 0; i < 4; i++) {
                 const uint32_t a = g4 * 4 + i;
-                v[i] = a < A ? *reinterpret_cast<const uint4*>(raw + a * 512 + s * 16) : make_uint4(0u, 0u, 0u, 0u);
+                v[i] = a < A ? *reinterpret_cast<const uint4*>(raw + a * rrow + s * 16) : make_uint4(0u, 0u, 0u, 0u);
             }
             half2 Z[4][4];
 #pragma unroll
@@ -227,18 +240,116 @@ __device__ __forceinline__ void build_operand(const uint8_t* raw, uint8_t* op, u
     }
 }
 
-// Window sum of 16 per-beam values over I = 2^LOGI adjacent lanes by a butterfly
-// reduce-scatter: after min(LOGI, 4) halving rounds each lane holds the window sums
-// of 16 >> min(LOGI, 4) consecutive beams starting at *first; the rest of the
-// rounds (I = 32) are a plain exchange.  Returns the number of values this lane
-// stores (0 for the duplicate half when I = 32).
-template <int LOGI>
-__device__ __forceinline__ int window_reduce(float (&v)[16], uint32_t lane, uint32_t* first) {
-    constexpr int RS = LOGI < 4 ? LOGI : 4;
+// R = 4, both polarisations in one pass.  Each sample word is split into two
+// half2 words with the polarisations in the two halves, RE = (p0 re, p1 re) and
+// IM = (p0 im, p1 im), read exactly as 1024 + (x + 128) = 1152 + x through the
+// 0x64 exponent byte (one XOR of the sign bits, two byte permutes).  The DFT then
+// runs in FP16 on the FMA pipe (the integer pipe issues at half rate): every
+// intermediate is an integer of magnitude < 2048, so all of it is exact, and the
+// 1152 biases cancel in differences or are removed together (x0 + x2 =
+// ((1024 + u0) - 2304) + (1024 + u2) with both steps exact).  A warp covers 16
+// spectra x 8 antennas (two 4-antenna groups): lanes 0-7 and 8-15 write the two
+// 8-byte halves of one 16-byte chunk for 8 rows with distinct swizzle slots, lanes
+// 16-31 the next 8 rows, so each 8-byte store is two conflict-free wavefronts.
+// Row k * 32 + s of an operand sits 4096 * k bytes after row s (the swizzle phase
+// depends on s only), so a task's addresses are fixed offsets computed once.
+struct R4Task {
+    uint32_t raw_off;  // a0 * rrow + s * 16 in the raw stage
+    uint32_t o_r, o_i; // operand offsets of (row s, K = a0) and (row s, K = KA + a0)
+    uint32_t nvalid;   // antennas a0 .. a0 + nvalid - 1 exist (0..4)
+};
+
+__device__ __forceinline__ R4Task r4_task(uint32_t wt, uint32_t lane, uint32_t A, uint32_t KA, uint32_t rrow) {
+    const uint32_t c = wt >> 1;
+    const uint32_t s = (wt & 1u) * 16u + (lane & 7u) + ((lane >> 4) << 3);
+    const uint32_t a0 = (2u * c + ((lane >> 3) & 1u)) * 4u;
+    R4Task t;
+    t.raw_off = a0 * rrow + s * 16u;
+    t.o_r = op_off(s, a0);
+    t.o_i = op_off(s, KA + a0);
+    t.nvalid = a0 < A ? min(4u, A - a0) : 0u;
+    return t;
+}
+
+__device__ __forceinline__ void r4_pair_task(const uint8_t* raw, uint32_t rrow, uint8_t* op0, uint8_t* op1,
+                                             const R4Task& t) {
+    const half2 h2304 = __halves2half2(__ushort_as_half(0x6880), __ushort_as_half(0x6880));  // 2304
+    uint2 out_r[2][4], out_i[2][4];  // [pol][k]
+    if (t.nvalid) {
+        half2 zr[4][4], zi[4][4];  // [antenna][k], halves = (pol 0, pol 1)
+        const uint8_t* src = raw + t.raw_off;
+#pragma unroll
+        for (uint32_t i = 0; i < 4; i++) {
+            const uint4 v = i < t.nvalid ? *reinterpret_cast<const uint4*>(src + i * rrow) : make_uint4(0u, 0u, 0u, 0u);
+            const uint32_t w[4] = {v.x ^ 0x80808080u, v.y ^ 0x80808080u, v.z ^ 0x80808080u, v.w ^ 0x80808080u};
+            half2 re[4], im[4];  // 1152 + x
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                re[j] = u2h(__byte_perm(w[j], 0x64646464u, 0x4240));
+                im[j] = u2h(__byte_perm(w[j], 0x64646464u, 0x4341));
+            }
+            const half2 aR = __hadd2(__hsub2(re[0], h2304), re[2]);  // x0 + x2
+            const half2 bR = __hadd2(__hsub2(re[1], h2304), re[3]);  // x1 + x3
+            const half2 cR = __hsub2(re[0], re[2]), dR = __hsub2(re[1], re[3]);
+            const half2 aI = __hadd2(__hsub2(im[0], h2304), im[2]);
+            const half2 bI = __hadd2(__hsub2(im[1], h2304), im[3]);
+            const half2 cI = __hsub2(im[0], im[2]), dI = __hsub2(im[1], im[3]);
+            zr[i][0] = __hsub2(aR, bR);  // x0 - x1 + x2 - x3
+            zi[i][0] = __hsub2(aI, bI);
+            zr[i][1] = __hsub2(cR, dI);  // x0 + i x1 - x2 - i x3
+            zi[i][1] = __hadd2(cI, dR);
+            zr[i][2] = __hadd2(aR, bR);  // x0 + x1 + x2 + x3
+            zi[i][2] = __hadd2(aI, bI);
+            zr[i][3] = __hadd2(cR, dI);  // x0 - i x1 - x2 + i x3
+            zi[i][3] = __hsub2(cI, dR);
+        }
+#pragma unroll
+        for (int p = 0; p < 2; p++) {
+            const uint32_t sel = p ? 0x7632u : 0x5410u;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                out_r[p][k].x = __byte_perm(h2u(zr[0][k]), h2u(zr[1][k]), sel);
+                out_r[p][k].y = __byte_perm(h2u(zr[2][k]), h2u(zr[3][k]), sel);
+                out_i[p][k].x = __byte_perm(h2u(zi[0][k]), h2u(zi[1][k]), sel);
+                out_i[p][k].y = __byte_perm(h2u(zi[2][k]), h2u(zi[3][k]), sel);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int p = 0; p < 2; p++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) out_r[p][k] = out_i[p][k] = make_uint2(0u, 0u);
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < 4; k++) {
+        *reinterpret_cast<uint2*>(op0 + t.o_r + k * 4096u) = out_r[0][k];
+        *reinterpret_cast<uint2*>(op0 + t.o_i + k * 4096u) = out_i[0][k];
+        *reinterpret_cast<uint2*>(op1 + t.o_r + k * 4096u) = out_r[1][k];
+        *reinterpret_cast<uint2*>(op1 + t.o_i + k * 4096u) = out_i[1][k];
+    }
+}
+
+// Both polarisations of one tile for R = 1 and 2: two single-polarisation passes.
+template <int R>
+__device__ __forceinline__ void build_operand_pair(const uint8_t* raw, uint32_t rrow, uint8_t* op0, uint8_t* op1, uint32_t A,
+                                                   uint32_t KA, uint32_t ct) {
+    build_operand<R>(raw, rrow, op0, A, KA, 0, ct);
+    build_operand<R>(raw, rrow, op1, A, KA, 1, ct);
+}
+
+// Window sum of NV per-beam values over I = 2^LOGI adjacent lanes by a butterfly
+// reduce-scatter: after min(LOGI, log2 NV) halving rounds each lane holds the
+// window sums of NV >> min(LOGI, log2 NV) consecutive beams starting at *first; the
+// remaining rounds (I > NV) are a plain exchange.  Returns the number of values
+// this lane stores (0 for the lanes that hold duplicates when I > NV).
+template <int NV, int LOGI>
+__device__ __forceinline__ int window_reduce(float (&v)[NV], uint32_t lane, uint32_t* first) {
+    constexpr int LOGNV = NV == 16 ? 4 : NV == 8 ? 3 : NV == 4 ? 2 : NV == 2 ? 1 : 0;
+    constexpr int RS = LOGI < LOGNV ? LOGI : LOGNV;
     uint32_t off = 0;
 #pragma unroll
     for (int s = 0; s < RS; s++) {
-        const int half = 16 >> (s + 1);
+        const int half = NV >> (s + 1);
         const bool upper = (lane >> s) & 1u;
 #pragma unroll
         for (int j = 0; j < half; j++) {
@@ -251,8 +362,8 @@ __device__ __forceinline__ int window_reduce(float (&v)[16], uint32_t lane, uint
 #pragma unroll
     for (int s = RS; s < LOGI; s++) v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1 << s);
     *first = off;
-    if (LOGI > 4 && ((lane >> 4) & 1u)) return 0;
-    return 16 >> RS;
+    if (LOGI > LOGNV && ((lane >> LOGNV) & ((1u << (LOGI > LOGNV ? LOGI - LOGNV : 0)) - 1u))) return 0;
+    return NV >> RS;
 }
 
 // ---- MMA issue ----------------------------------------------------------------
@@ -307,20 +418,33 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
     uint64_t* r_full = a_empty + AS;
     uint64_t* r_empty = r_full + RS;
     uint64_t* d_full = r_empty + RS;
-    uint64_t* d_empty = d_full + 2;
-    uint64_t* w_full = d_empty + 2;
+    uint64_t* d_empty = d_full + kMaxAcc;
+    uint64_t* w_full = d_empty + kMaxAcc;
     uint64_t* w_empty = w_full + 1;
-    uint64_t* fin = w_empty + 1;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fin + 1);
+    uint64_t* fin = w_empty + 1;  // one per MMA issuer
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fin + 2);
     volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     volatile int never = 0;  // abort flag that is never raised (drain waits)
     // Accumulator columns per polarisation: [re | im] (2 NB), or with hi/lo stacked
-    // along N [hi re | hi im | lo re | lo im] (4 NB); two tiles in flight.
+    // along N [hi re | hi im | lo re | lo im] (4 NB).
     const uint32_t d_cols = (g.stacked ? 4u : 2u) * NB;
-    const uint32_t need_cols = 4 * d_cols;
+    // Accumulator buffers (tiles in flight between MMA and epilogue): as many as
+    // fit the 512 TMEM columns, at most kMaxAcc.
+    const uint32_t nacc = min((uint32_t)kMaxAcc, 512u / (2u * d_cols));
+    const uint32_t need_cols = nacc * 2u * d_cols;
     const uint32_t tmem_cols = need_cols <= 32 ? 32 : need_cols <= 64 ? 64 : need_cols <= 128 ? 128 : need_cols <= 256 ? 256 : 512;
+    // Pair mode: the converter builds both polarisations of a tile in one pass and
+    // signals them together on the second stage of the pair.
+    const bool pair = AS >= 4 && (AS & 1u) == 0;
+
+    // Two MMA issuers (warp 0 and the last warp, lane 0 each) take alternate tiles
+    // when the operand ring holds an even number of tile pairs and the accumulator
+    // count is even, so that every barrier is only ever used by one issuer.  An
+    // issue of tcgen05.mma holds its thread for about the MMA's duration, so one
+    // issuer's waits and commits overlap the other's MMAs.
+    const uint32_t nis = (pair && ((AS / 2) & 1u) == 0 && (nacc & 1u) == 0) ? 2u : 1u;
 
     if (threadIdx.x == 0) {
         for (uint32_t i = 0; i < AS; i++) {
@@ -331,13 +455,14 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
             mbar_init(&r_full[i], 1);
             mbar_init(&r_empty[i], kConvWarps);
         }
-        for (int i = 0; i < 2; i++) {
+        for (uint32_t i = 0; i < nacc; i++) {
             mbar_init(&d_full[i], 1);
             mbar_init(&d_empty[i], kEpiWarps);
         }
         mbar_init(w_full, 1);
-        mbar_init(w_empty, 1);
-        mbar_init(fin, 1);
+        mbar_init(w_empty, nis);
+        mbar_init(&fin[0], 1);
+        mbar_init(&fin[1], 1);
         *abort = 0;
         fence_mbar_init();
     }
@@ -350,15 +475,26 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    // This CTA's contiguous range of (channel, time-tile) tiles.
-    const uint64_t per = (g.total_tiles + gridDim.x - 1) / gridDim.x;
+    // This CTA's contiguous range of (channel, time-tile) tiles, a whole number of
+    // raw stages (tiles per channel is a multiple of raw_tiles).
+    const uint64_t per = ((g.total_tiles + gridDim.x - 1) / gridDim.x + g.raw_tiles - 1) / g.raw_tiles * g.raw_tiles;
     const uint64_t L0 = (uint64_t)blockIdx.x * per;
     const uint64_t L1 = min(g.total_tiles, L0 + per);
     const uint32_t tpc = g.tiles_per_ch;
+    const int issuer = warp == 0 ? 0 : (warp == kWarps - 1 ? 1 : -1);
 
-    if (warp == 0) {
-        // ---------------- MMA issuer ----------------
-        if (lane == 0 && L0 < L1) {
+    if (issuer >= 0) {
+        // ---------------- MMA issuers ----------------
+        const uint32_t j = (uint32_t)issuer;
+        // The whole warp runs the loop and the waits (a lone active lane beside lanes
+        // parked at the final barrier progressed slowly); lane 0 issues the MMAs and
+        // the commits, which track that thread's MMAs.
+        auto wait_all = [&](uint64_t* bar, uint32_t parity, unsigned code) -> bool {
+            const bool w = __all_sync(0xffffffffu, mbar_wait(bar, parity, abort, kWaitBudget));
+            if (!w && lane == 0) record_abort(abort, code);
+            return w;
+        };
+        if (L0 < L1 && j < nis) {
             const uint32_t idesc = idesc_f16(kM, d_cols);
             const uint64_t w_desc = smem_desc_sw128(smem_u32(w_smem));
             const uint64_t a_desc = smem_desc_sw128(smem_u32(a_smem));
@@ -368,43 +504,66 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
             //   stacked: (2 KA / 64) column blocks of 4 NB rows;
             //   KA = 64: two (hi, lo) x three NB-row blocks; KA = 32: two x one 2 NB-row block.
             const uint32_t wpol16 = g.stacked ? (2 * KA / 64) * 4 * nb16 : (KA == 64 ? 6 * nb16 : 4 * nb16);
-            uint32_t as = 0, aph = 0, db = 0, dph = 0, wph = 0;
+            // This issuer's first tile is local tile j: operand stage 2 j (pair mode)
+            // or 0, accumulator j; both advance by nis tiles per own tile.
+            uint32_t as = pair ? 2 * j : 0, aph = 0, db = j, dph = 0, wph = 0;
+            uint32_t tt = (uint32_t)(L0 % tpc);  // time tile within the channel, stepped below
             bool ok = true;
-            for (uint64_t L = L0; L < L1 && ok; L++) {
-                const uint32_t tt = (uint32_t)(L % tpc);
+            uint32_t i = 0;
+            for (uint64_t L = L0; L < L1 && ok; L++, i++) {
                 if (L == L0 || tt == 0) {
-                    if (!mbar_wait(w_full, wph, abort, kWaitBudget)) { record_abort(abort, 1); ok = false; break; }
+                    if (!wait_all(w_full, wph, 1)) { ok = false; break; }
                 }
-                if (!mbar_wait(&d_empty[db], dph ^ 1, abort, kWaitBudget)) { record_abort(abort, 3); ok = false; break; }
-                for (uint32_t p = 0; p < 2; p++) {
-                    if (!mbar_wait(&a_full[as], aph, abort, kWaitBudget)) { record_abort(abort, 2); ok = false; break; }
-                    tc_fence_after();
-                    const uint64_t ad = a_desc + (uint64_t)(as * op16);
-                    const uint64_t wd = w_desc + (uint64_t)(p * wpol16);
-                    const uint32_t d = tmem + db * (2 * d_cols) + p * d_cols;
-                    if (g.stacked) {
-                        if (KA == 64) issue_stacked<8>(d, ad, wd, 4 * nb16, idesc);
-                        else issue_stacked<4>(d, ad, wd, 4 * nb16, idesc);
-                    } else if (KA == 64) {
-                        issue_ka64(d, ad, wd, nb16, idesc);
-                    } else {
-                        issue_ka32(d, ad, wd, nb16, idesc);
+                if ((i % nis) == j) {
+                    if (!wait_all(&d_empty[db], dph ^ 1, 3)) { ok = false; break; }
+                    const uint32_t np = pair ? 1u : 2u;  // operand handshakes per tile
+                    for (uint32_t h = 0; h < np; h++) {
+                        // pair mode: the converter signals both polarisation stages on as + 1
+                        const uint32_t sig = pair ? as + 1 : as;
+                        if (!wait_all(&a_full[sig], aph, 2)) { ok = false; break; }
+                        tc_fence_after();
+                        if (lane == 0) {
+                            for (uint32_t p = pair ? 0u : h; p < (pair ? 2u : h + 1); p++) {
+                                const uint64_t ad = a_desc + (uint64_t)((as + (pair ? p : 0u)) * op16);
+                                const uint64_t wd = w_desc + (uint64_t)(p * wpol16);
+                                const uint32_t d = tmem + db * (2 * d_cols) + p * d_cols;
+                                if (g.stacked) {
+                                    if (KA == 64) issue_stacked<8>(d, ad, wd, 4 * nb16, idesc);
+                                    else issue_stacked<4>(d, ad, wd, 4 * nb16, idesc);
+                                } else if (KA == 64) {
+                                    issue_ka64(d, ad, wd, nb16, idesc);
+                                } else {
+                                    issue_ka32(d, ad, wd, nb16, idesc);
+                                }
+                            }
+                            mma_commit(&a_empty[sig]);
+                        }
+                        __syncwarp();
+                        as += pair ? 2u * nis : 1u;
+                        if (as >= AS) { as -= AS; aph ^= 1; }
                     }
-                    mma_commit(&a_empty[as]);
-                    if (++as == AS) { as = 0; aph ^= 1; }
+                    if (!ok) break;
+                    if (lane == 0) mma_commit(&d_full[db]);
+                    __syncwarp();
+                    db += nis;
+                    if (db >= nacc) { db -= nacc; dph ^= 1; }
                 }
-                if (!ok) break;
-                mma_commit(&d_full[db]);
+                // Every issuer releases the phasor image at the end of each channel
+                // segment (the barrier counts one arrival per issuer).
                 if (tt == tpc - 1 || L + 1 == L1) {
-                    mma_commit(w_empty);
+                    if (lane == 0) mma_commit(w_empty);
+                    __syncwarp();
                     wph ^= 1;
                 }
-                if (++db == 2) { db = 0; dph ^= 1; }
+                if (++tt == tpc) tt = 0;
             }
             // Drain every MMA issued by this thread before TMEM is released
             // (bounded, but not cut short by the abort flag).
-            mma_commit(fin);
-            if (!mbar_wait(fin, 0, &never, kWaitBudget)) record_abort(abort, 4);
+            if (lane == 0) {
+                mma_commit(&fin[j]);
+                if (!mbar_wait(&fin[j], 0, &never, kWaitBudget)) record_abort(abort, 4);
+            }
+            __syncwarp();
         }
     } else if (warp == 1) {
         // ---------------- loader: phasor image + raw CI8 tiles (bulk copies) ----------------
@@ -412,8 +571,13 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
             uint32_t rs = 0, rph = 0, wph = 0;
             bool w_issued = false;
             uint32_t issued_mask = 0, issued_par = 0;  // per raw stage: issued?, parity of last issue
-            for (uint64_t L = L0; L < L1; L++) {
-                const uint32_t f = (uint32_t)(L / tpc), tt = (uint32_t)(L % tpc);
+            // One raw stage = raw_tiles consecutive tiles of one channel, loaded as one or
+            // two TMA boxes of up to 256 samples x 1 channel x A antennas (rows of
+            // raw_row bytes per antenna: 512-byte rows per tile leave DRAM bandwidth
+            // unused, 1-2 KB rows do not).
+            const uint32_t RT = g.raw_tiles, box = g.raw_row / 4, nbox = RT * kM / box;
+            uint32_t f = (uint32_t)(L0 / tpc), tt = (uint32_t)(L0 % tpc);  // stepped below
+            for (uint64_t L = L0; L < L1; L += RT) {
                 int ok = 1;
                 if (L == L0 || tt == 0) {
                     if (lane == 0) {
@@ -433,10 +597,11 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
                 if (lane == 0) {
                     ok = mbar_wait(&r_empty[rs], rph ^ 1, abort, kWaitBudget);
                     if (ok) {
-                        // One tensor load per tile: 128 samples x 1 channel x A antennas,
-                        // landing antenna-major (512 bytes per antenna) in the raw stage.
-                        mbar_arrive_expect_tx(&r_full[rs], g.A * 512u);
-                        tma_load_3d(r_smem + (size_t)rs * g.raw_bytes, &tmap, (int)(tt * kM), (int)f, 0, &r_full[rs]);
+                        mbar_arrive_expect_tx(&r_full[rs], g.A * 512u * RT);
+                        uint8_t* dst = r_smem + (size_t)rs * g.raw_bytes;
+                        for (uint32_t b = 0; b < nbox; b++)
+                            tma_load_3d(dst + (size_t)b * g.A * g.raw_row, &tmap, (int)(tt * kM + b * box), (int)f, 0,
+                                        &r_full[rs]);
                     } else {
                         record_abort(abort, 9);
                     }
@@ -446,6 +611,8 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
                 issued_mask |= 1u << rs;
                 issued_par = (issued_par & ~(1u << rs)) | (rph << rs);
                 if (++rs == RS) { rs = 0; rph ^= 1; }
+                tt += RT;
+                if (tt == tpc) { tt = 0; f++; }
             }
             // Every bulk copy this warp issued must land before the CTA exits.
             if (lane == 0) {
@@ -459,60 +626,63 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
     } else if (warp < 2 + kEpiWarps) {
         // ---------------- epilogue ----------------
         constexpr uint32_t I = 1u << LOGI;
-        const uint32_t q = warp & 3;  // TMEM lane quarter this warp may access
+        const uint32_t q = warp & 3;               // TMEM lane quarter this warp may access
+        const uint32_t hw = (warp - 2) >> 2;       // which share of the beams
+        const uint32_t nbh = NB / kEpiGroups;      // beams per warp, a multiple of 8
         constexpr uint32_t rows_per_k = kM / R;
         const uint32_t row = 32 * q + lane;
         const uint32_t k = row / rows_per_k;
         const uint32_t s_local = row - k * rows_per_k;
+        const uint64_t bstride = (uint64_t)g.F * R * g.U;
         uint32_t db = 0, dph = 0;
+        uint32_t f = (uint32_t)(L0 / tpc), tt = (uint32_t)(L0 % tpc);  // stepped below
         for (uint64_t L = L0; L < L1; L++) {
             if (!mbar_wait(&d_full[db], dph, abort, kWaitBudget)) { record_abort(abort, 7); break; }
             tc_fence_after();
-            const uint32_t f = (uint32_t)(L / tpc), tt = (uint32_t)(L % tpc);
             const uint32_t u = (tt * rows_per_k + s_local) / I;
             const uint32_t lane_addr = tmem + ((32 * q) << 16) + db * (2 * d_cols);
             float* obase = g.out + ((uint64_t)f * R + k) * g.U + u;
-            const uint64_t bstride = (uint64_t)g.F * R * g.U;
-            for (uint32_t bc = 0; bc < NB; bc += 16) {
-                float pw[16];
+            constexpr int CH = 16 / kEpiGroups;  // beams per TMEM load (16 or 8)
+            for (uint32_t bc = hw * nbh; bc < (hw + 1) * nbh; bc += CH) {
+                float pw[CH];
                 if (g.stacked) {
                     // per polarisation: (hi + lo) re, (hi + lo) im
 #pragma unroll
-                    for (int j = 0; j < 16; j++) pw[j] = 0.f;
+                    for (int j = 0; j < CH; j++) pw[j] = 0.f;
 #pragma unroll
                     for (uint32_t p = 0; p < 2; p++) {
-                        uint32_t hr[16], hi[16], lr[16], li[16];
+                        uint32_t hr[CH], hi[CH], lr[CH], li[CH];
                         const uint32_t pa = lane_addr + p * d_cols + bc;
-                        tmem_ld16(pa, hr);
-                        tmem_ld16(pa + NB, hi);
-                        tmem_ld16(pa + 2 * NB, lr);
-                        tmem_ld16(pa + 3 * NB, li);
+                        tmem_ld(pa, hr);
+                        tmem_ld(pa + NB, hi);
+                        tmem_ld(pa + 2 * NB, lr);
+                        tmem_ld(pa + 3 * NB, li);
                         tmem_ld_wait();
 #pragma unroll
-                        for (int j = 0; j < 16; j++) {
+                        for (int j = 0; j < CH; j++) {
                             const float a = __uint_as_float(hr[j]) + __uint_as_float(lr[j]);
                             const float b = __uint_as_float(hi[j]) + __uint_as_float(li[j]);
                             pw[j] = fmaf(a, a, fmaf(b, b, pw[j]));
                         }
                     }
                 } else {
-                    uint32_t r0[16], i0[16], r1[16], i1[16];
-                    tmem_ld16(lane_addr + bc, r0);
-                    tmem_ld16(lane_addr + NB + bc, i0);
-                    tmem_ld16(lane_addr + 2 * NB + bc, r1);
-                    tmem_ld16(lane_addr + 3 * NB + bc, i1);
+                    uint32_t r0[CH], i0[CH], r1[CH], i1[CH];
+                    tmem_ld(lane_addr + bc, r0);
+                    tmem_ld(lane_addr + NB + bc, i0);
+                    tmem_ld(lane_addr + 2 * NB + bc, r1);
+                    tmem_ld(lane_addr + 3 * NB + bc, i1);
                     tmem_ld_wait();
 #pragma unroll
-                    for (int j = 0; j < 16; j++) {
+                    for (int j = 0; j < CH; j++) {
                         const float a0 = __uint_as_float(r0[j]), b0 = __uint_as_float(i0[j]);
                         const float a1 = __uint_as_float(r1[j]), b1 = __uint_as_float(i1[j]);
                         pw[j] = fmaf(a0, a0, fmaf(b0, b0, fmaf(a1, a1, b1 * b1)));
                     }
                 }
                 uint32_t first;
-                const int cnt = window_reduce<LOGI>(pw, lane, &first);
+                const int cnt = window_reduce<CH, LOGI>(pw, lane, &first);
 #pragma unroll
-                for (int j = 0; j < 16; j++) {
+                for (int j = 0; j < CH; j++) {
                     if (j < cnt) {
                         const uint32_t b = bc + first + j;
                         if (b < g.beams) obase[b * bstride] = pw[j];
@@ -522,28 +692,68 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&d_empty[db]);
-            if (++db == 2) { db = 0; dph ^= 1; }
+            if (++db == nacc) { db = 0; dph ^= 1; }
+            if (++tt == tpc) { tt = 0; f++; }
         }
-    } else {
+    } else if (warp < 2 + kEpiWarps + kConvWarps) {
         // ---------------- operand build ----------------
-        const uint32_t ct = threadIdx.x - (2 + kEpiWarps) * 32;  // 0..255
+        const uint32_t ct = threadIdx.x - (2 + kEpiWarps) * 32;  // 0 .. 32 kConvWarps - 1
+        // R = 4 pair mode: this warp's warp-tasks (KA / 4 of them over kConvWarps warps),
+        // addresses fixed for the kernel
+        constexpr uint32_t kMaxT4 = kMaxKA / 4 / kConvWarps;
+        const uint32_t nt4 = KA / 4 / kConvWarps;
+        R4Task t4[kMaxT4];
+        if constexpr (R == 4) {
+#pragma unroll
+            for (uint32_t i = 0; i < kMaxT4; i++) t4[i] = r4_task((ct >> 5) + i * kConvWarps, lane, g.A, KA, g.raw_row);
+        }
         uint32_t rs = 0, rph = 0, as = 0, aph = 0;
+        uint32_t sub = 0;  // tile within the raw stage (CTA ranges are stage-aligned)
         bool ok = true;
         for (uint64_t L = L0; L < L1 && ok; L++) {
-            if (!mbar_wait(&r_full[rs], rph, abort, kWaitBudget)) { record_abort(abort, 11); break; }
-            const uint8_t* raw = r_smem + (size_t)rs * g.raw_bytes;
-            for (int p = 0; p < 2; p++) {
-                if (!mbar_wait(&a_empty[as], aph ^ 1, abort, kWaitBudget)) { record_abort(abort, 8); ok = false; break; }
-                build_operand<R>(raw, a_smem + (size_t)as * op_bytes, g.A, KA, p, ct);
+            if (sub == 0) {
+                if (!mbar_wait(&r_full[rs], rph, abort, kWaitBudget)) { record_abort(abort, 11); break; }
+            }
+            // this tile inside the stage: box (sub * 128 / box), column (sub * 128 % box)
+            const uint32_t sb = sub * kM, box = g.raw_row / 4;
+            const uint8_t* raw = r_smem + (size_t)rs * g.raw_bytes + (sb / box) * g.A * g.raw_row + (sb % box) * 4u;
+            if (pair) {
+                // Both polarisations in one pass into stages as, as + 1 (AS is even).
+                if (!mbar_wait(&a_empty[as + 1], aph ^ 1, abort, kWaitBudget)) {
+                    record_abort(abort, 8);
+                    break;
+                }
+                uint8_t* op0 = a_smem + (size_t)as * op_bytes;
+                uint8_t* op1 = op0 + op_bytes;
+                if constexpr (R == 4) {
+#pragma unroll
+                    for (uint32_t i = 0; i < kMaxT4; i++)
+                        if (i < nt4) r4_pair_task(raw, g.raw_row, op0, op1, t4[i]);
+                } else {
+                    build_operand_pair<R>(raw, g.raw_row, op0, op1, g.A, KA, ct);
+                }
                 fence_proxy_async_smem();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&a_full[as]);
-                if (++as == AS) { as = 0; aph ^= 1; }
+                if (lane == 0) mbar_arrive(&a_full[as + 1]);
+                as += 2;
+                if (as == AS) { as = 0; aph ^= 1; }
+            } else {
+                for (int p = 0; p < 2; p++) {
+                    if (!mbar_wait(&a_empty[as], aph ^ 1, abort, kWaitBudget)) { record_abort(abort, 8); ok = false; break; }
+                    build_operand<R>(raw, g.raw_row, a_smem + (size_t)as * op_bytes, g.A, KA, p, ct);
+                    fence_proxy_async_smem();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&a_full[as]);
+                    if (++as == AS) { as = 0; aph ^= 1; }
+                }
+                if (!ok) break;
             }
-            if (!ok) break;
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&r_empty[rs]);
-            if (++rs == RS) { rs = 0; rph ^= 1; }
+            if (++sub == g.raw_tiles) {
+                sub = 0;
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&r_empty[rs]);
+                if (++rs == RS) { rs = 0; rph ^= 1; }
+            }
         }
     }
 
@@ -630,10 +840,12 @@ __global__ void __launch_bounds__(256) tc_prepare_kernel(const float2* __restric
 
 struct TcShape {
     uint32_t NB, KA, nchunks, img_bytes, raw_bytes, a_stages, r_stages, stacked;
+    uint32_t raw_tiles, raw_row;
     size_t smem;
 };
 
-bool tc_shape(uint64_t B, uint64_t A, TcShape& s) {
+// T = 0 sizes only the phasor image (the ring layout needs the tiles per channel).
+bool tc_shape(uint64_t B, uint64_t A, TcShape& s, uint64_t T = 0) {
     if (A == 0 || A > kMaxKA || B == 0) return false;
     const uint64_t bc = B < (uint64_t)kMaxNB ? B : (uint64_t)kMaxNB;
     s.NB = (uint32_t)((bc + 15) / 16 * 16);
@@ -645,11 +857,39 @@ bool tc_shape(uint64_t B, uint64_t A, TcShape& s) {
     s.img_bytes = s.stacked ? (2 * s.KA / 64) * 1024u * s.NB : (s.KA == 64 ? 1536u : 1024u) * s.NB;
     s.raw_bytes = (uint32_t)A * 512u;
     const size_t op = (2ull * s.KA / 64) * 16384;   // one polarisation's operand
-    const size_t fixed = s.img_bytes + 256 + 1024;  // barriers, TMEM slot, abort flag, alignment slack
+    // barriers (2 x 8 operand + 2 x 8 raw + 2 x 4 accumulator + 3, 8 bytes each),
+    // TMEM slot and abort flag, alignment slack
+    const size_t fixed = s.img_bytes + 512 + 1024;
     const size_t limit = 227 * 1024;
-    uint32_t as = 4, rs = 6;
+    // Two-tile raw stages (1 KB per antenna row) when the channel's tile count is even
+    // and one of these rings fits: four operand tile pairs and two raw stages (the
+    // operand build runs up to four tiles ahead of the MMAs), else two pairs and
+    // four or three raw stages.
+    const uint64_t tpc = T / kM;
+    if (T && tpc % 2 == 0) {
+        const size_t raw2 = (size_t)A * 1024u;
+        const uint32_t cand[][2] = {{8, 2}, {4, 4}, {4, 3}};
+        for (const auto& c : cand) {
+            if (fixed + c[0] * op + c[1] * raw2 <= limit) {
+                s.raw_tiles = 2;
+                s.raw_row = 1024;
+                s.raw_bytes = (uint32_t)raw2;
+                s.a_stages = c[0];
+                s.r_stages = c[1];
+                s.smem = fixed + c[0] * op + c[1] * raw2;
+                return true;
+            }
+        }
+    }
+    s.raw_tiles = 1;
+    s.raw_row = 512;
+    // Deepest rings that fit: operand stages in pairs (one per polarisation) down to
+    // four, raw stages down to three, then both down to the minimum.
+    uint32_t as = kMaxStages, rs = 6;
     while (fixed + as * op + rs * (size_t)s.raw_bytes > limit) {
-        if (rs > 2 && rs >= as) rs--;
+        if (rs > 3 && (rs > as / 2 || as <= 4)) rs--;
+        else if (as > 4) as -= 2;
+        else if (rs > 2) rs--;
         else if (as > 2) as--;
         else if (rs > 1) rs--;
         else return false;
@@ -663,8 +903,8 @@ bool tc_shape(uint64_t B, uint64_t A, TcShape& s) {
 using TcKernel = void (*)(const TcArgs, const CUtensorMap);
 
 // Tensor map of the CI8 voltages seen as uint32 samples [A][F][T] (one 4-byte
-// word = both polarisations of one sample); box = 128 samples x 1 channel x A.
-int encode_voltage_map(CUtensorMap* tm, const void* in, uint64_t A, uint64_t F, uint64_t T) {
+// word = both polarisations of one sample); box = `box` samples x 1 channel x A.
+int encode_voltage_map(CUtensorMap* tm, const void* in, uint64_t A, uint64_t F, uint64_t T, uint32_t box_t) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     static std::mutex mu;
     {
@@ -681,7 +921,7 @@ int encode_voltage_map(CUtensorMap* tm, const void* in, uint64_t A, uint64_t F, 
     }
     const cuuint64_t dims[3] = {T, F, A};
     const cuuint64_t strides[2] = {T * 4, F * T * 4};
-    const cuuint32_t box[3] = {(cuuint32_t)kM, 1, (cuuint32_t)A};
+    const cuuint32_t box[3] = {box_t, 1, (cuuint32_t)A};
     const cuuint32_t estr[3] = {1, 1, 1};
     const CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, const_cast<void*>(in), dims, strides, box, estr,
                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -762,13 +1002,13 @@ extern "C" int blade_beamform_detect_tc(const void* in, const void* plan, void* 
     if (!aligned16(in) || !aligned16(plan) || (reinterpret_cast<uintptr_t>(out) & 3))
         return set_error(BLADE_ERROR, "blade_beamform_detect_tc: input and plan must be 16-byte aligned");
     TcShape s;
-    tc_shape(B, A, s);
+    tc_shape(B, A, s, T);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const TcKernel fn = pick_kernel(rate, integration);
     if (int rc = ensure_smem(reinterpret_cast<const void*>(fn), s.smem)) return rc;
     const uint32_t U = (uint32_t)(T / (rate * integration));
     CUtensorMap tmap;
-    if (int rc = encode_voltage_map(&tmap, in, A, F, T)) return rc;
+    if (int rc = encode_voltage_map(&tmap, in, A, F, T, s.raw_row / 4)) return rc;
     for (uint32_t c = 0; c < s.nchunks; c++) {
         TcArgs g;
         g.in = static_cast<const uint8_t*>(in);
@@ -786,11 +1026,16 @@ extern "C" int blade_beamform_detect_tc(const void* in, const void* plan, void* 
         g.r_stages = s.r_stages;
         g.img_bytes = s.img_bytes;
         g.raw_bytes = s.raw_bytes;
+        g.raw_tiles = s.raw_tiles;
+        g.raw_row = s.raw_row;
         g.stacked = s.stacked;
         g.tiles_per_ch = (uint32_t)(T / kM);
         g.total_tiles = (uint64_t)F * (T / kM);
-        uint64_t grid = (uint64_t)sm_count();
-        if (grid > g.total_tiles) grid = g.total_tiles;
+        // Whole raw stages per CTA (the kernel rounds its share up to raw_tiles); no
+        // CTA is left without tiles.
+        const uint64_t sms = (uint64_t)sm_count();
+        const uint64_t per = ((g.total_tiles + sms - 1) / sms + s.raw_tiles - 1) / s.raw_tiles * s.raw_tiles;
+        const uint64_t grid = (g.total_tiles + per - 1) / per;
         fn<<<(unsigned)grid, kThreads, s.smem, st>>>(g, tmap);
         if (int rc = check_launch("blade_beamform_detect_tc")) return rc;
     }
