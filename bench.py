@@ -14,7 +14,12 @@ also carries the ingest rate, the plain FP32 CUDA-core path on the same block,
 the dense 64 x 64 workload (A = B = 64, F = 256, T = 8192, I = 8) for both
 paths, the roofline of the dominant kernel, the CPU baseline (the reference's
 numpy formulas, FP64, on a bounded channel sample) and the end-to-end rate
-through the public Runner API with host buffers.
+through the public Runner API with host buffers.  Three further legs cover the
+other measured workloads: the high-resolution spectrometer (A = 1, F = 64,
+T = 2^20, Cast -> Channelizer(65536) -> Polarizer -> Detector I = 8), the small
+block's launch latency eager against one CUDA graph (A = 20, F = 96, T = 256,
+B = 8), and the forward + adjoint step of the Stokes loss (A = 28, B = 1,
+F = 192, T = 2048, CF32); --skip-extra leaves them out.
 
 Multi-GPU (torchrun): weak scaling, every rank owns its own 192-channel band
 (frequency sharding, no data-path collective); time = max over ranks.
@@ -298,6 +303,166 @@ def e2e_runner(w, steps, warmup, world):
     return max_over_ranks(ms, world), h2d, d2h
 
 
+SPECTRO = dict(A=1, F=64, T=1 << 20, P=2, R=65536, I=8)
+SMALL = dict(A=20, F=96, T=256, P=2, B=8, R=1, I=4)
+ADJ = dict(A=28, F=192, T=2048, P=2, B=1)
+
+
+def spectrometer(steps, warmup):
+    """High-resolution spectrometer on one dual-polarisation stream, module by module:
+    Cast<CI8,CF32> -> Channelizer(rate 65536) -> Polarizer -> Detector(Stokes-I, I=8)
+    (A=1, F=64, T=2^20, P=2).  Per-kernel device times and GB/s against each kernel's
+    own bytes, and the chain's rate against the fused minimum (CI8 in + Stokes-I out)."""
+    from blade_b200 import _lib
+
+    lib = _lib.load()
+    A, F, T, P, R, I = (SPECTRO[k] for k in ("A", "F", "T", "P", "R", "I"))
+    s = torch.cuda.current_stream()
+    sh = s.cuda_stream
+    g = torch.Generator(device="cuda").manual_seed(1004)
+    x = (torch.randn((A, F, T, P, 2), generator=g, device="cuda") * 8).round_().clamp_(-127, 127).to(torch.int8)
+    xf = torch.empty((A, F, T, P), dtype=torch.complex64, device="cuda")
+    yc = torch.empty((A, F * R, T // R, P), dtype=torch.complex64, device="cuda")
+    ws_bytes = int(lib.blade_channelize_workspace_size(A, F, T, P, R))
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device="cuda")
+    out = torch.empty((A, F * R, T // (R * I), 1), dtype=torch.float32, device="cuda")
+    n = A * F * T * P
+    kernels = [
+        ("cast", lambda: _lib.call("blade_cast", _lib.CI8, _lib.CF32, x.data_ptr(), xf.data_ptr(), n, sh), 2 * n + 8 * n),
+        # four-step FFT: input read, workspace written and read back, output written
+        ("channelize", lambda: _lib.call("blade_channelize", xf.data_ptr(), yc.data_ptr(),
+                                         ws.data_ptr() if ws_bytes else None, A, F, T, P, R, sh),
+         (32 if ws_bytes else 16) * n),
+        ("polarize", lambda: _lib.call("blade_polarize", _lib.CF32, yc.data_ptr(), yc.data_ptr(), A * F * T, sh), 16 * n),
+        ("detect", lambda: _lib.call("blade_detect", yc.data_ptr(), out.data_ptr(), A, F * R, T // R, P, I, 1, sh),
+         8 * n + 4 * (n // P) // I),
+    ]
+    for _ in range(warmup):
+        for _, fn, _ in kernels:
+            fn()
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(kernels) + 1)] for _ in range(steps)]
+    for k in range(steps):
+        ev[k][0].record(s)
+        for j, (_, fn, _) in enumerate(kernels):
+            fn()
+            ev[k][j + 1].record(s)
+    torch.cuda.synchronize()
+    per = [sum(ev[k][j].elapsed_time(ev[k][j + 1]) for k in range(steps)) / steps for j in range(len(kernels))]
+    total = sum(per)
+    fused_min = 2 * n + 4 * (n // P) // I
+    _, _, peak_kind = load_peaks()
+    hbm = load_peaks()[0]
+    res = {"workload": "A=1 F=64 T=2^20 P=2, Cast->Channelizer(65536)->Polarizer->Detector(Stokes-I, I=8)",
+           "ms_per_step": round(total, 4),
+           "fused_min_bytes": fused_min,
+           "gbs_vs_fused_min": round(fused_min / (total * 1e-3) / 1e9, 1),
+           "fft_gflops": round(5 * n * np.log2(R) / (per[1] * 1e-3) / 1e9, 1),
+           "kernels": {}}
+    for (name, _, nbytes), ms in zip(kernels, per):
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        res["kernels"][name] = {"ms": round(ms, 4), "bytes": nbytes, "gbs": round(gbs, 1),
+                                "frac_of_hbm": round(gbs / hbm, 3)}
+    res["hbm_peak_gbs"] = hbm
+    del x, xf, yc, ws, out
+    return res
+
+
+def small_block_latency(calls):
+    """Small ATA block (A=20 F=96 T=256 P=2 B=8, I=4): Cast -> Beamformer(FP32) -> Detector,
+    three launches per call, eager against one CUDA graph replay.  Reports the host
+    wall time of one call waited to completion (latency) and the device time per call
+    when calls are issued back to back (throughput)."""
+    from blade_b200 import _lib
+
+    _lib.load()
+    A, F, T, P, B, I = (SMALL[k] for k in ("A", "F", "T", "P", "B", "I"))
+    g = torch.Generator(device="cuda").manual_seed(1001)
+    x = (torch.randn((A, F, T, P, 2), generator=g, device="cuda") * 8).round_().clamp_(-127, 127).to(torch.int8)
+    ph = torch.polar(torch.ones((B, A, F, 1, P), device="cuda"),
+                     torch.rand((B, A, F, 1, P), generator=g, device="cuda") * 6.283185307)
+    xf = torch.empty((A, F, T, P), dtype=torch.complex64, device="cuda")
+    y = torch.empty((B, F, T, P), dtype=torch.complex64, device="cuda")
+    out = torch.empty((B, F, T // I, 1), dtype=torch.float32, device="cuda")
+    side = torch.cuda.Stream()
+
+    def call(sh):
+        _lib.call("blade_cast", _lib.CI8, _lib.CF32, x.data_ptr(), xf.data_ptr(), A * F * T * P, sh)
+        _lib.call("blade_beamform_f32", xf.data_ptr(), ph.data_ptr(), y.data_ptr(), B, A, F, T, P, 0, 0, sh)
+        _lib.call("blade_detect", y.data_ptr(), out.data_ptr(), B, F, T, P, I, 1, sh)
+
+    with torch.cuda.stream(side):
+        sh = side.cuda_stream
+        for _ in range(10):
+            call(sh)
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=side):
+            call(torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+
+        def measure(fn):
+            lat = []
+            for _ in range(calls):
+                t = time.perf_counter()
+                fn()
+                side.synchronize()
+                lat.append(time.perf_counter() - t)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(side)
+            for _ in range(calls):
+                fn()
+            e1.record(side)
+            side.synchronize()
+            return float(np.median(lat)) * 1e6, e0.elapsed_time(e1) * 1e3 / calls
+
+        eager_lat, eager_dev = measure(lambda: call(sh))
+        graph_lat, graph_dev = measure(graph.replay)
+    del graph
+    mac = 4 * B * A * F * T * P
+    return {"workload": "A=20 F=96 T=256 P=2 B=8 I=4, Cast->Beamformer(FP32)->Detector, 3 launches",
+            "eager_us_per_call": round(eager_lat, 2), "graph_us_per_call": round(graph_lat, 2),
+            "eager_device_us_per_call": round(eager_dev, 2), "graph_device_us_per_call": round(graph_dev, 2),
+            "graph_tmacs": round(mac / (graph_dev * 1e-6) / 1e12, 4)}
+
+
+def adjoint_step(steps, warmup):
+    """Forward + adjoint of the Stokes loss (A=28 B=1 F=192 T=2048 P=2, CF32 voltages):
+    one blade_beamform_detect_adjoint call recomputes the beam tile by tile and returns
+    the loss and dL/dconj(w); HBM-bound on the 176 MB voltage read."""
+    from blade_b200 import _lib
+
+    _lib.load()
+    A, F, T, P, B = (ADJ[k] for k in ("A", "F", "T", "P", "B"))
+    s = torch.cuda.current_stream()
+    sh = s.cuda_stream
+    g = torch.Generator(device="cuda").manual_seed(1005)
+    x = torch.complex(torch.randn((A, F, T, P), generator=g, device="cuda"),
+                      torch.randn((A, F, T, P), generator=g, device="cuda"))
+    ph = torch.polar(torch.ones((B, A, F, 1, P), device="cuda"),
+                     torch.rand((B, A, F, 1, P), generator=g, device="cuda") * 6.283185307)
+    grad = torch.empty_like(ph)
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    for _ in range(warmup):
+        _lib.call("blade_beamform_detect_adjoint", x.data_ptr(), ph.data_ptr(), grad.data_ptr(), loss.data_ptr(),
+                  B, A, F, T, P, sh)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(steps):
+        _lib.call("blade_beamform_detect_adjoint", x.data_ptr(), ph.data_ptr(), grad.data_ptr(), loss.data_ptr(),
+                  B, A, F, T, P, sh)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    nbytes = A * F * T * P * 8 + 2 * B * A * F * P * 8
+    hbm = load_peaks()[0]
+    return {"workload": "A=28 B=1 F=192 T=2048 P=2 CF32, Stokes loss + dL/dconj(w)",
+            "ms_per_step": round(ms, 4), "gbs": round(nbytes / (ms * 1e-3) / 1e9, 1),
+            "frac_of_hbm": round(nbytes / (ms * 1e-3) / 1e9 / hbm, 3),
+            "macs_fwd_plus_adj": 2 * 4 * B * A * F * T * P}
+
+
 def cpu_baseline(w, out_gpu, budget_s=10.0):
     """The reference's numpy formulas (FP64 oracle restatement) on a bounded
     channel sample of the same block, on every host core; also checks the GPU
@@ -351,6 +516,12 @@ def run_ours(args):
         dense_agree = float((dout_tc - dout_f32).norm() / dout_f32.norm())
         del xd, phd, dout_tc, dout_f32
         torch.cuda.synchronize()
+        extra = {}
+        if not args.skip_extra and world == 1:
+            extra["spectrometer"] = spectrometer(max(3, args.steps // 6), args.warmup)
+            extra["small_block_latency"] = small_block_latency(200)
+            extra["adjoint"] = adjoint_step(max(5, args.steps // 2), args.warmup)
+        torch.cuda.synchronize()
     clocks = clk.summary()
     if rank != 0:
         if world > 1:
@@ -401,6 +572,7 @@ def run_ours(args):
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
     }
+    line.update(extra)
     print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
@@ -466,6 +638,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--skip-extra", action="store_true",
+                    help="skip the spectrometer, small-block latency and adjoint legs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

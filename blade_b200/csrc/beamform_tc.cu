@@ -772,67 +772,93 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
 //            [hi: b -> (Wr | -Wi), NB + b -> (Wi | Wr) ; lo: the same],
 //   KA = 64, NB > 32: per (p, h) three blocks of NB rows x 64 K: [-Wi | Wr | Wi],
 //   KA = 32, NB > 32: per (p, h) one block of 2 NB rows: b -> [Wr | -Wi], NB + b -> [Wi | Wr].
-__device__ __forceinline__ void put_half(uint8_t* blk, uint32_t row, uint32_t k, __half v) {
-    *reinterpret_cast<__half*>(blk + sw128_off(row, (k >> 3) & 7u) + (k & 7u) * 2u) = v;
+// One thread writes the 16-byte chunks of one (chunk c, channel f, polarisation p,
+// beam row nb, 8-antenna group j) for hi and lo: 8 phasors in, 8 or 12 chunk
+// stores out.  Consecutive threads take consecutive channels, so the phasor loads
+// of a warp are 16 bytes apart.
+__device__ __forceinline__ uint4 pack8(const __half (&v)[8]) {
+    uint4 u;
+    u.x = (uint32_t)__half_as_ushort(v[0]) | ((uint32_t)__half_as_ushort(v[1]) << 16);
+    u.y = (uint32_t)__half_as_ushort(v[2]) | ((uint32_t)__half_as_ushort(v[3]) << 16);
+    u.z = (uint32_t)__half_as_ushort(v[4]) | ((uint32_t)__half_as_ushort(v[5]) << 16);
+    u.w = (uint32_t)__half_as_ushort(v[6]) | ((uint32_t)__half_as_ushort(v[7]) << 16);
+    return u;
 }
 
-// K index k_total over several 64-wide column blocks of `rows` rows each.
-__device__ __forceinline__ void put_half_k(uint8_t* base, uint32_t rows, uint32_t row, uint32_t k_total, __half v) {
-    put_half(base + (k_total >> 6) * rows * 128u, row, k_total & 63u, v);
+// 16-byte chunk holding K elements [k_total, k_total + 8) of `row` in a stack of
+// 64-wide column blocks of `rows` rows each.
+__device__ __forceinline__ void put_chunk(uint8_t* base, uint32_t rows, uint32_t row, uint32_t k_total, uint4 v) {
+    *reinterpret_cast<uint4*>(base + (k_total >> 6) * rows * 128u + sw128_off(row, (k_total >> 3) & 7u)) = v;
 }
 
 __global__ void __launch_bounds__(256) tc_prepare_kernel(const float2* __restrict__ ph, uint8_t* __restrict__ plan,
                                                          uint32_t B, uint32_t A, uint32_t F, uint32_t NB,
                                                          uint32_t KA, uint32_t nchunks, uint32_t img_bytes,
                                                          uint32_t stacked) {
-    const uint64_t n = (uint64_t)nchunks * F * 2 * NB * KA;
+    const uint32_t groups = KA / 8;
+    const uint32_t n = nchunks * F * 2u * NB * groups;
     const uint32_t ph_bytes = (KA == 64 ? 3u : 2u) * NB * 128u;
     const uint32_t pol_stacked = (2 * KA / 64) * 4 * NB * 128u;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t a = (uint32_t)(i % KA);
-        uint64_t r = i / KA;
-        const uint32_t nb = (uint32_t)(r % NB);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t r = i;
+        const uint32_t f = r % F;
+        r /= F;
+        const uint32_t p = r & 1u;
+        r >>= 1;
+        const uint32_t nb = r % NB;
         r /= NB;
-        const uint32_t p = (uint32_t)(r % 2);
-        r /= 2;
-        const uint32_t f = (uint32_t)(r % F);
-        const uint32_t c = (uint32_t)(r / F);
+        const uint32_t j = r % groups;
+        const uint32_t c = r / groups;
         const uint32_t b = c * kMaxNB + nb;
-        float wr = 0.f, wi = 0.f;
-        if (a < A && b < B) {
-            const float2 w = ph[((uint64_t)(b * (uint64_t)A + a) * F + f) * 2 + p];
-            wr = w.x;
-            wi = w.y;
+        // hi = rn(w), lo = rn(w - hi) per component; padded antennas and beams are 0
+        __half rh[8], ih[8], rl[8], il[8], nih[8], nil[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const uint32_t a = j * 8 + e;
+            float wr = 0.f, wi = 0.f;
+            if (a < A && b < B) {
+                const float2 w = ph[((uint64_t)(b * (uint64_t)A + a) * F + f) * 2 + p];
+                wr = w.x;
+                wi = w.y;
+            }
+            rh[e] = __float2half_rn(wr);
+            ih[e] = __float2half_rn(wi);
+            rl[e] = __float2half_rn(wr - __half2float(rh[e]));
+            il[e] = __float2half_rn(wi - __half2float(ih[e]));
+            nih[e] = __hneg(ih[e]);
+            nil[e] = __hneg(il[e]);
         }
-        const __half rh = __float2half_rn(wr), ih = __float2half_rn(wi);
-        const __half rl = __float2half_rn(wr - __half2float(rh)), il = __float2half_rn(wi - __half2float(ih));
+        const uint32_t k0 = j * 8;
         if (stacked) {
+            // per p, (2 KA / 64) column blocks of 4 NB rows:
+            //   hi: row nb -> [Wr | -Wi], row NB + nb -> [Wi | Wr]; lo: the same at rows + 2 NB
             uint8_t* base = plan + ((uint64_t)c * F + f) * img_bytes + (uint64_t)p * pol_stacked;
             const uint32_t rows = 4 * NB;
-            for (uint32_t h = 0; h < 2; h++) {
-                const __half re = h ? rl : rh, im = h ? il : ih;
-                const uint32_t rr = h * 2 * NB + nb, ri = h * 2 * NB + NB + nb;
-                put_half_k(base, rows, rr, a, re);                // Re-output row, Xr part:  Wr
-                put_half_k(base, rows, rr, KA + a, __hneg(im));   // Re-output row, Xi part: -Wi
-                put_half_k(base, rows, ri, a, im);                // Im-output row, Xr part:  Wi
-                put_half_k(base, rows, ri, KA + a, re);           // Im-output row, Xi part:  Wr
-            }
+            put_chunk(base, rows, nb, k0, pack8(rh));
+            put_chunk(base, rows, nb, KA + k0, pack8(nih));
+            put_chunk(base, rows, NB + nb, k0, pack8(ih));
+            put_chunk(base, rows, NB + nb, KA + k0, pack8(rh));
+            put_chunk(base, rows, 2 * NB + nb, k0, pack8(rl));
+            put_chunk(base, rows, 2 * NB + nb, KA + k0, pack8(nil));
+            put_chunk(base, rows, 3 * NB + nb, k0, pack8(il));
+            put_chunk(base, rows, 3 * NB + nb, KA + k0, pack8(rl));
             continue;
         }
         uint8_t* base = plan + ((uint64_t)c * F + f) * img_bytes + (uint64_t)p * 2 * ph_bytes;
         for (int h = 0; h < 2; h++) {
             uint8_t* blk = base + h * ph_bytes;
-            const __half re = h ? rl : rh, im = h ? il : ih;
+            const uint4 re = pack8(h ? rl : rh), im = pack8(h ? il : ih), nim = pack8(h ? nil : nih);
             if (KA == 64) {
-                put_half(blk, nb, a, __hneg(im));                 // block 0: -Wi
-                put_half(blk + NB * 128u, nb, a, re);             // block 1:  Wr
-                put_half(blk + 2u * NB * 128u, nb, a, im);        // block 2:  Wi
+                // three blocks of NB rows x 64 K: [-Wi | Wr | Wi]
+                put_chunk(blk, NB, nb, k0, nim);
+                put_chunk(blk + NB * 128u, NB, nb, k0, re);
+                put_chunk(blk + 2u * NB * 128u, NB, nb, k0, im);
             } else {
-                put_half(blk, nb, a, re);                         // row b,      K < 32:  Wr
-                put_half(blk, nb, 32u + a, __hneg(im));           // row b,      K >= 32: -Wi
-                put_half(blk, NB + nb, a, im);                    // row NB + b, K < 32:  Wi
-                put_half(blk, NB + nb, 32u + a, re);              // row NB + b, K >= 32: Wr
+                // one block of 2 NB rows x 64 K: row nb -> [Wr | -Wi], row NB + nb -> [Wi | Wr]
+                put_chunk(blk, 2 * NB, nb, k0, re);
+                put_chunk(blk, 2 * NB, nb, 32u + k0, nim);
+                put_chunk(blk, 2 * NB, NB + nb, k0, im);
+                put_chunk(blk, 2 * NB, NB + nb, 32u + k0, re);
             }
         }
     }
@@ -971,7 +997,8 @@ extern "C" int blade_beamform_tc_prepare(const void* phasors, void* plan, uint64
     if (F == 0) return BLADE_SUCCESS;
     if (!phasors || !plan) return set_error(BLADE_ERROR, "blade_beamform_tc_prepare: null buffer");
     if (!aligned16(plan)) return set_error(BLADE_ERROR, "blade_beamform_tc_prepare: plan must be 16-byte aligned");
-    const uint64_t n = (uint64_t)s.nchunks * F * 2 * s.NB * s.KA;
+    const uint64_t n = (uint64_t)s.nchunks * F * 2 * s.NB * (s.KA / 8);
+    if (n > 0xFFFFFFFFull) return set_error(BLADE_ERROR, "blade_beamform_tc_prepare: too many channels");
     tc_prepare_kernel<<<grid_for(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         static_cast<const float2*>(phasors), static_cast<uint8_t*>(plan), (uint32_t)B, (uint32_t)A, (uint32_t)F,
         s.NB, s.KA, s.nchunks, s.img_bytes, s.stacked);

@@ -47,6 +47,33 @@ __global__ void __launch_bounds__(256) cast_vec_kernel(const IT* __restrict__ in
     }
 }
 
+// Widening casts (output wider than input): each thread writes one 16-byte output
+// vector per step from a 2-, 4- or 8-byte input piece, so both the loads and the
+// stores of a warp are contiguous.
+template <int BYTES> struct Piece;
+template <> struct Piece<2> { using T = uint16_t; };
+template <> struct Piece<4> { using T = uint32_t; };
+template <> struct Piece<8> { using T = uint2; };
+
+template <typename IT, typename OT>
+__global__ void __launch_bounds__(256) cast_widen_kernel(const IT* __restrict__ in, OT* __restrict__ out,
+                                                         uint64_t nvec) {
+    constexpr int VO = 16 / sizeof(OT);            // elements per output vector
+    constexpr int IB = VO * (int)sizeof(IT);       // input bytes per vector: 2, 4 or 8
+    using PT = typename Piece<IB>::T;
+    const PT* pin = reinterpret_cast<const PT*>(in);
+    uint4* pout = reinterpret_cast<uint4*>(out);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nvec; i += stride) {
+        const PT raw = __ldg(pin + i);
+        const IT* src = reinterpret_cast<const IT*>(&raw);
+        alignas(16) OT dst[VO];
+#pragma unroll
+        for (int k = 0; k < VO; k++) dst[k] = Conv<IT, OT>::f(src[k]);
+        pout[i] = *reinterpret_cast<const uint4*>(dst);
+    }
+}
+
 template <typename IT, typename OT>
 __global__ void cast_scalar_kernel(const IT* __restrict__ in, OT* __restrict__ out, uint64_t begin,
                                    uint64_t n) {
@@ -62,6 +89,18 @@ int launch_cast(const void* vin, void* vout, uint64_t n, cudaStream_t s) {
     if (n == 0) return BLADE_SUCCESS;
     constexpr int V = 16 / sizeof(IT);
     uint64_t done = 0;
+    if constexpr (sizeof(OT) > sizeof(IT)) {
+        constexpr int VO = 16 / sizeof(OT);
+        if (aligned16(out) && (reinterpret_cast<uintptr_t>(in) % (VO * sizeof(IT))) == 0) {
+            const uint64_t nvec = n / VO;
+            if (nvec) {
+                cast_widen_kernel<IT, OT><<<grid_for(nvec, 256), 256, 0, s>>>(in, out, nvec);
+                done = nvec * VO;
+            }
+            if (done < n) cast_scalar_kernel<IT, OT><<<grid_for(n - done, 256), 256, 0, s>>>(in, out, done, n);
+            return check_launch("blade_cast");
+        }
+    }
     if (aligned16(in) && (reinterpret_cast<uintptr_t>(out) % (V * sizeof(OT) >= 16 ? 16 : V * sizeof(OT))) == 0) {
         uint64_t nvec = n / V;
         if (nvec) {

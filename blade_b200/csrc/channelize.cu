@@ -28,10 +28,16 @@ constexpr uint32_t kSmallMax = 4096;
 struct Plan {
     int n;       // number of passes
     int r[20];   // radix of each pass
+    int log2n;   // log2 N when N is a power of two, else -1 (shift/mask indexing)
 };
 
 bool make_plan(uint64_t N, Plan& p) {
     p.n = 0;
+    p.log2n = -1;
+    if ((N & (N - 1)) == 0) {
+        p.log2n = 0;
+        while ((1ull << p.log2n) < N) p.log2n++;
+    }
     uint64_t n = N;
     while (n % 8 == 0) { p.r[p.n++] = 8; n /= 8; }
     while (n % 4 == 0) { p.r[p.n++] = 4; n /= 4; }
@@ -72,16 +78,18 @@ __device__ __forceinline__ void dft4(float2& a, float2& b, float2& c, float2& d)
 // W holds exp(-2 pi i m / N), m < N.  Returns the buffer holding the result.
 __device__ float2* stockham(float2* b0, float2* b1, const float2* W, uint32_t N, uint32_t G, const Plan& plan) {
     uint32_t Ns = 1;
+    const bool pow2 = plan.log2n >= 0;
     for (int ps = 0; ps < plan.n; ps++) {
         const uint32_t R = plan.r[ps];
         const uint32_t NR = N / R;
         const uint32_t total = G * NR;
         const uint32_t tws = N / (Ns * R);  // twiddle index stride
+        const uint32_t lnr = pow2 ? (uint32_t)plan.log2n - (R == 8 ? 3u : R == 4 ? 2u : 1u) : 0u;
         for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) {
-            const uint32_t g = e / NR, j = e - g * NR;
+            const uint32_t g = pow2 ? e >> lnr : e / NR, j = e - g * NR;
             const float2* src = b0 + g * N;
             float2* dst = b1 + g * N;
-            const uint32_t jm = j % Ns;
+            const uint32_t jm = pow2 ? (j & (Ns - 1u)) : j % Ns;
             const uint32_t idxD = (j - jm) * R + jm;
             const uint32_t tw = jm * tws;
             if (R == 8) {
@@ -197,9 +205,10 @@ __global__ void __launch_bounds__(kThreads) fft_small_kernel(const float2* __res
 //   X[k1 + N1 k2] = sum_j2 w_N2^(j2 k2) [ w_N^(j2 k1) sum_j1 x[N2 j1 + j2] w_N1^(j1 k1) ]
 
 constexpr uint32_t kJB = 16;  // columns per CTA in the first step
+constexpr int kThreads4 = 512;  // threads of the four-step kernels (one CTA per SM for the column step)
 
 template <int P>
-__global__ void __launch_bounds__(kThreads) fft_cols_kernel(const float2* __restrict__ in, float2* __restrict__ ws,
+__global__ void __launch_bounds__(kThreads4) fft_cols_kernel(const float2* __restrict__ in, float2* __restrict__ ws,
                                                             uint32_t A, uint32_t F, uint32_t T, uint32_t N1,
                                                             uint32_t N2, Plan plan) {
     extern __shared__ __align__(16) float2 smem[];
@@ -233,7 +242,8 @@ __global__ void __launch_bounds__(kThreads) fft_cols_kernel(const float2* __rest
         for (uint32_t e = threadIdx.x; e < G * N1; e += blockDim.x) {
             const uint32_t jl = e % kJB, k1 = (e / kJB) % N1, p = e / (kJB * N1);
             const uint32_t j2 = c0 + jl;
-            const uint32_t m = (uint32_t)(((uint64_t)j2 * k1) % N);
+            const uint32_t jk = j2 * k1;  // < N1 N2 <= 2^24
+            const uint32_t m = (N & (N - 1u)) == 0 ? (jk & (N - 1u)) : jk % N;
             const float2 v = cmul(res[(p * kJB + jl) * N1 + k1], twiddle(m, N));
             ws[((batch * P + p) * N1 + k1) * (uint64_t)N2 + j2] = v;
         }
@@ -242,7 +252,7 @@ __global__ void __launch_bounds__(kThreads) fft_cols_kernel(const float2* __rest
 }
 
 template <int P>
-__global__ void __launch_bounds__(kThreads) fft_rows_kernel(const float2* __restrict__ ws, float2* __restrict__ out,
+__global__ void __launch_bounds__(kThreads4) fft_rows_kernel(const float2* __restrict__ ws, float2* __restrict__ out,
                                                             uint32_t A, uint32_t F, uint32_t T, uint32_t N1,
                                                             uint32_t N2, uint32_t SB, Plan plan) {
     extern __shared__ __align__(16) float2 smem[];
@@ -284,6 +294,216 @@ __global__ void __launch_bounds__(kThreads) fft_rows_kernel(const float2* __rest
             }
         }
         __syncthreads();
+    }
+}
+
+// ---- rate 65536 = 256 x 256: register-blocked four-step --------------------
+// A 256-point FFT runs on 16 threads: n = 16 n1 + n2, k = k1 + 16 k2,
+//   X[k1 + 16 k2] = sum_n2 w16^(n2 k2) [ w256^(n2 k1) sum_n1 x[16 n1 + n2] w16^(n1 k1) ],
+// thread n2 does the inner 16-point DFT in registers, the products go through
+// shared memory once, thread k1 does the outer one.  A 16-point DFT is 4 x 4:
+// four DFT-4s over n1 (stride 4), the w16 twiddles, four DFT-4s over n2.
+__device__ __forceinline__ void dft16(float2 (&v)[16]) {
+    // v[n], n = 4 a + b -> in place, result index k = c + 4 d at position c + 4 d
+#pragma unroll
+    for (int b = 0; b < 4; b++) dft4(v[b], v[4 + b], v[8 + b], v[12 + b]);  // over a: U[b][c] at v[4 c + b]
+    const float c1 = 0.92387953251128676f, s1 = 0.38268343236508977f, h = 0.70710678118654752f;
+    // w16^(b c) for b, c in 1..3: exponents 1, 2, 3, 2, 4, 6, 3, 6, 9
+    v[4 + 1] = cmul(v[4 + 1], make_float2(c1, -s1));   // b 1, c 1: w^1
+    v[8 + 1] = cmul(v[8 + 1], make_float2(h, -h));     // b 1, c 2: w^2
+    v[12 + 1] = cmul(v[12 + 1], make_float2(s1, -c1)); // b 1, c 3: w^3
+    v[4 + 2] = cmul(v[4 + 2], make_float2(h, -h));     // b 2, c 1: w^2
+    v[8 + 2] = mul_mi(v[8 + 2]);                       // b 2, c 2: w^4 = -i
+    v[12 + 2] = cmul(v[12 + 2], make_float2(-h, -h));  // b 2, c 3: w^6
+    v[4 + 3] = cmul(v[4 + 3], make_float2(s1, -c1));   // b 3, c 1: w^3
+    v[8 + 3] = cmul(v[8 + 3], make_float2(-h, -h));    // b 3, c 2: w^6
+    v[12 + 3] = cmul(v[12 + 3], make_float2(-c1, s1)); // b 3, c 3: w^9
+#pragma unroll
+    for (int c = 0; c < 4; c++) dft4(v[4 * c + 0], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);  // over b: X[c + 4 d] at v[4 c + d]
+    // reorder: position 4 c + d holds X[c + 4 d]; transpose the 4 x 4 in registers
+    float2 t[16];
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+#pragma unroll
+        for (int d = 0; d < 4; d++) t[c + 4 * d] = v[4 * c + d];
+#pragma unroll
+    for (int k = 0; k < 16; k++) v[k] = t[k];
+}
+
+// Column step for N = 65536 (N1 = N2 = 256): one CTA = one (a, f, s) spectrum, 16
+// consecutive columns j2, both polarisations (32 FFTs x 16 threads = 512 threads).
+// Output ws[((batch P + p) 256 + k1) 256 + j2] = w65536^(j2 k1) FFT256_j1(x[256 j1 + j2])[k1].
+// Padded stride of a 256-point column / row in shared memory: odd, so columns
+// read or written side by side fall in different banks, and >= 16 * 17 so the
+// 16 x 16 exchange can use row stride 17 (conflict-free in both directions).
+constexpr uint32_t kLd = 273;
+constexpr uint32_t kZ = 17;
+
+// v[k] *= w^k for k = 0..15 by recurrence from w (15 complex products, relative
+// error a few FP32 ulps): replaces 16 strided, bank-conflicting table lookups.
+__device__ __forceinline__ void twiddle_run(float2 (&v)[16], float2 base, float2 w) {
+    float2 acc = base;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        v[k] = cmul(v[k], acc);
+        acc = cmul(acc, w);
+    }
+}
+
+template <int P>
+__global__ void __launch_bounds__(512) fft256_cols_kernel(const float2* __restrict__ in, float2* __restrict__ ws,
+                                                          uint64_t batches) {
+    extern __shared__ __align__(16) float2 sm[];
+    float2* tile = sm;                   // [p][jc][kLd]   (16 P columns)
+    float2* w256 = tile + 16 * P * kLd;  // w256^m, m < 256
+    float2* wlo = w256 + 256;            // w65536^m, m < 256
+    for (uint32_t m = threadIdx.x; m < 256; m += blockDim.x) {
+        w256[m] = twiddle(m, 256);
+        wlo[m] = twiddle(m, 65536);
+    }
+    const uint32_t t = threadIdx.x & 15u, jc = (threadIdx.x >> 4) & 15u, p = threadIdx.x >> 8;
+    const bool active = p < (uint32_t)P;
+    float2* col = tile + (p * 16 + jc) * kLd;
+    for (uint64_t grp = blockIdx.x; grp < batches * 16; grp += gridDim.x) {
+        const uint64_t batch = grp >> 4;
+        const uint32_t c0 = (uint32_t)(grp & 15u) * 16u;
+        const float2* src = in + batch * 65536ull * P;
+        __syncthreads();
+        // coalesced load: rows j1 of 16 columns x P (256 B per row for P = 2); all of a
+        // thread's loads are issued before any shared-memory store
+        constexpr uint32_t kPer = 256u * 16u / 512u;  // 8 per thread
+        if (P == 2) {
+            float4 ld[kPer];
+#pragma unroll
+            for (uint32_t u = 0; u < kPer; u++) {
+                const uint32_t e = threadIdx.x + u * 512u, j1 = e >> 4, jl = e & 15u;
+                ld[u] = ldg_nc_f4(src + 2 * ((uint64_t)j1 * 256u + c0 + jl));
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < kPer; u++) {
+                const uint32_t e = threadIdx.x + u * 512u, j1 = e >> 4, jl = e & 15u;
+                tile[(0 * 16 + jl) * kLd + j1] = make_float2(ld[u].x, ld[u].y);
+                tile[(1 * 16 + jl) * kLd + j1] = make_float2(ld[u].z, ld[u].w);
+            }
+        } else {
+            float2 ld[kPer];
+#pragma unroll
+            for (uint32_t u = 0; u < kPer; u++) {
+                const uint32_t e = threadIdx.x + u * 512u, j1 = e >> 4, jl = e & 15u;
+                ld[u] = src[(uint64_t)j1 * 256u + c0 + jl];
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < kPer; u++) {
+                const uint32_t e = threadIdx.x + u * 512u, j1 = e >> 4, jl = e & 15u;
+                tile[jl * kLd + j1] = ld[u];
+            }
+        }
+        __syncthreads();
+        float2 v[16];
+        if (active) {
+#pragma unroll
+            for (int n1 = 0; n1 < 16; n1++) v[n1] = col[16 * n1 + t];  // thread n2 = t
+            dft16(v);
+            twiddle_run(v, make_float2(1.f, 0.f), w256[t]);  // w256^(t k1)
+        }
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int k1 = 0; k1 < 16; k1++) col[kZ * t + k1] = v[k1];  // Z[n2 = t][k1]
+        }
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int n2 = 0; n2 < 16; n2++) v[n2] = col[kZ * n2 + t];  // thread k1 = t
+            dft16(v);  // X[t + 16 k2]
+            // inter-step twiddle w65536^(j2 (t + 16 k2)): base w^(j2 t), step w^(16 j2),
+            // each from the two-level table w256^(m >> 8) w65536^(m & 255)
+            const uint32_t j2 = c0 + jc;
+            const uint32_t m0 = j2 * t, m1 = (16u * j2) & 65535u;
+            twiddle_run(v, cmul(w256[m0 >> 8], wlo[m0 & 255u]), cmul(w256[m1 >> 8], wlo[m1 & 255u]));
+        }
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int k2 = 0; k2 < 16; k2++) col[t + 16 * k2] = v[k2];  // col[k1] = result, k1 = t + 16 k2
+        }
+        __syncthreads();
+        // coalesced store: for each (p, k1), 16 consecutive j2
+        for (uint32_t e = threadIdx.x; e < (uint32_t)P * 256u * 16u; e += blockDim.x) {
+            const uint32_t jl = e & 15u, k1 = (e >> 4) & 255u, pp = e >> 12;
+            ws[((batch * P + pp) * 256u + k1) * 256ull + c0 + jl] = tile[(pp * 16 + jl) * kLd + k1];
+        }
+    }
+}
+
+// Row step for N = 65536: one CTA = one (a, f) and one k1, all S spectra x P
+// polarisations (S P <= 32 FFTs, 16 threads each).  X[k1 + 256 k2] goes to the
+// fftshifted channel k1 + 256 k2 + N/2 (mod N) of [A, F*N, S, P].
+template <int P>
+__global__ void __launch_bounds__(512) fft256_rows_kernel(const float2* __restrict__ ws, float2* __restrict__ out,
+                                                          uint64_t AF, uint32_t S) {
+    extern __shared__ __align__(16) float2 sm[];
+    float2* rows = sm;                     // [q = s P + p][kLd], q < S P <= 32
+    float2* w256 = rows + 32 * kLd;
+    for (uint32_t m = threadIdx.x; m < 256; m += blockDim.x) w256[m] = twiddle(m, 256);
+    const uint32_t t = threadIdx.x & 15u, q = threadIdx.x >> 4;
+    const uint32_t nq = S * P;
+    const bool active = q < nq;
+    float2* row = rows + q * kLd;
+    for (uint64_t grp = blockIdx.x; grp < AF * 256u; grp += gridDim.x) {
+        const uint64_t af = grp >> 8;
+        const uint32_t k1 = (uint32_t)(grp & 255u);
+        __syncthreads();
+        {
+            // rows (s, p, k1) of 256 contiguous values; pairs of values per 16-byte load,
+            // all of a thread's loads issued before the shared-memory stores
+            float4 ld[8];
+#pragma unroll
+            for (uint32_t u = 0; u < 8; u++) {
+                const uint32_t e = threadIdx.x + u * 512u, j2 = (e & 127u) * 2u, qq = e >> 7;
+                if (qq < nq)
+                    ld[u] = ldg_nc_f4(ws + (((af * S) * P + qq) * 256u + k1) * 256ull + j2);
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < 8; u++) {
+                const uint32_t e = threadIdx.x + u * 512u, j2 = (e & 127u) * 2u, qq = e >> 7;
+                if (qq < nq) {
+                    rows[qq * kLd + j2] = make_float2(ld[u].x, ld[u].y);
+                    rows[qq * kLd + j2 + 1] = make_float2(ld[u].z, ld[u].w);
+                }
+            }
+        }
+        __syncthreads();
+        float2 v[16];
+        if (active) {
+#pragma unroll
+            for (int n1 = 0; n1 < 16; n1++) v[n1] = row[16 * n1 + t];
+            dft16(v);
+            twiddle_run(v, make_float2(1.f, 0.f), w256[t]);
+        }
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < 16; k++) row[kZ * t + k] = v[k];
+        }
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int n2 = 0; n2 < 16; n2++) v[n2] = row[kZ * n2 + t];
+            dft16(v);  // X2[t + 16 c] = final X[k1 + 256 (t + 16 c)]
+        }
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int c = 0; c < 16; c++) row[t + 16 * c] = v[c];
+        }
+        __syncthreads();
+        // out[(af N + kout) S + s][p], kout = (k1 + 256 k2 + 32768) mod 65536; (s, p) fastest
+        for (uint32_t e = threadIdx.x; e < 256u * nq; e += blockDim.x) {
+            const uint32_t qq = e % nq, k2 = e / nq;
+            const uint32_t kout = (k1 + 256u * k2 + 32768u) & 65535u;
+            out[((af * 65536ull + kout) * S) * P + qq] = rows[qq * kLd + k2];
+        }
     }
 }
 
@@ -376,6 +596,25 @@ extern "C" int blade_channelize(const void* in, void* out, void* workspace, uint
     if (!make_plan(N1, p1) || !make_plan(N2, p2))
         return set_error(BLADE_ERROR, "blade_channelize: rate %llu has a prime factor above 61", (unsigned long long)rate);
     float2* ws = static_cast<float2*>(workspace);
+    if (N1 == 256 && N2 == 256 && S * P <= 32) {
+        const uint64_t batches = A * F * S;
+        const size_t sm1 = (16 * P * kLd + 512) * sizeof(float2), sm2 = (32 * kLd + 256) * sizeof(float2);
+        const uint64_t cap = (uint64_t)sm_count() * 2;
+        const uint64_t g1 = batches * 16, g2 = A * F * 256;
+        int rc;
+        if (P == 2) {
+            if ((rc = prepare_smem(fft256_cols_kernel<2>, sm1))) return rc;
+            if ((rc = prepare_smem(fft256_rows_kernel<2>, sm2))) return rc;
+            fft256_cols_kernel<2><<<(unsigned)(g1 < cap ? g1 : cap), 512, sm1, s>>>(src, ws, batches);
+            fft256_rows_kernel<2><<<(unsigned)(g2 < cap ? g2 : cap), 512, sm2, s>>>(ws, dst, A * F, (uint32_t)S);
+        } else {
+            if ((rc = prepare_smem(fft256_cols_kernel<1>, sm1))) return rc;
+            if ((rc = prepare_smem(fft256_rows_kernel<1>, sm2))) return rc;
+            fft256_cols_kernel<1><<<(unsigned)(g1 < cap ? g1 : cap), 512, sm1, s>>>(src, ws, batches);
+            fft256_rows_kernel<1><<<(unsigned)(g2 < cap ? g2 : cap), 512, sm2, s>>>(ws, dst, A * F, (uint32_t)S);
+        }
+        return check_launch("blade_channelize");
+    }
     const size_t smem1 = (N1 + 2 * kJB * P * N1) * sizeof(float2);
     uint64_t SB2 = 4096 / (N2 * P);
     if (SB2 < 1) SB2 = 1;
@@ -388,16 +627,16 @@ extern "C" int blade_channelize(const void* in, void* out, void* workspace, uint
     if (P == 2) {
         if ((rc = prepare_smem(fft_cols_kernel<2>, smem1))) return rc;
         if ((rc = prepare_smem(fft_rows_kernel<2>, smem2))) return rc;
-        fft_cols_kernel<2><<<(unsigned)(g1 < cap ? g1 : cap), kThreads, smem1, s>>>(
+        fft_cols_kernel<2><<<(unsigned)(g1 < cap ? g1 : cap), kThreads4, smem1, s>>>(
             src, ws, (uint32_t)A, (uint32_t)F, (uint32_t)T, (uint32_t)N1, (uint32_t)N2, p1);
-        fft_rows_kernel<2><<<(unsigned)(g2 < cap ? g2 : cap), kThreads, smem2, s>>>(
+        fft_rows_kernel<2><<<(unsigned)(g2 < cap ? g2 : cap), kThreads4, smem2, s>>>(
             ws, dst, (uint32_t)A, (uint32_t)F, (uint32_t)T, (uint32_t)N1, (uint32_t)N2, (uint32_t)SB2, p2);
     } else {
         if ((rc = prepare_smem(fft_cols_kernel<1>, smem1))) return rc;
         if ((rc = prepare_smem(fft_rows_kernel<1>, smem2))) return rc;
-        fft_cols_kernel<1><<<(unsigned)(g1 < cap ? g1 : cap), kThreads, smem1, s>>>(
+        fft_cols_kernel<1><<<(unsigned)(g1 < cap ? g1 : cap), kThreads4, smem1, s>>>(
             src, ws, (uint32_t)A, (uint32_t)F, (uint32_t)T, (uint32_t)N1, (uint32_t)N2, p1);
-        fft_rows_kernel<1><<<(unsigned)(g2 < cap ? g2 : cap), kThreads, smem2, s>>>(
+        fft_rows_kernel<1><<<(unsigned)(g2 < cap ? g2 : cap), kThreads4, smem2, s>>>(
             ws, dst, (uint32_t)A, (uint32_t)F, (uint32_t)T, (uint32_t)N1, (uint32_t)N2, (uint32_t)SB2, p2);
     }
     return check_launch("blade_channelize");

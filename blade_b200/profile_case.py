@@ -4,8 +4,11 @@
 
 Workloads: ata-small (A=20 F=96 T=256 B=8 rate 1 I=4), ata-production
 (A=28 F=192 T=8192 B=16 rate 4 I=4), dense-64x64 (A=64 F=256 T=8192 B=64 rate 1
-I=8).  Paths: tc (phasor split + tensor-core chain), f32 (fused FP32 chain),
-modules (Cast -> Beamformer -> Channelizer -> Detector, one launch each).
+I=8), spectrometer (A=1 F=64 T=2^20, rate 65536, I=8, no beamformer) and
+spectrometer-small (the same with F=16, for full profiler captures).  Paths: tc
+(phasor split + tensor-core chain), f32 (fused FP32 chain), modules (Cast ->
+Beamformer -> Channelizer -> Detector, one launch each; for the spectrometer
+Cast -> Channelizer -> Polarizer -> Detector).
 Inputs are seeded synthetic CI8 voltages and phasors, created on the device.
 """
 
@@ -22,6 +25,8 @@ WORKLOADS = {
     "ata-small": dict(A=20, F=96, T=256, B=8, R=1, I=4),
     "ata-production": dict(A=28, F=192, T=8192, B=16, R=4, I=4),
     "dense-64x64": dict(A=64, F=256, T=8192, B=64, R=1, I=8),
+    "spectrometer": dict(A=1, F=64, T=1 << 20, B=0, R=65536, I=8),
+    "spectrometer-small": dict(A=1, F=16, T=1 << 20, B=0, R=65536, I=8),
 }
 
 
@@ -37,6 +42,19 @@ def main():
     s = torch.cuda.current_stream().cuda_stream
     g = torch.Generator(device="cuda").manual_seed(7)
     x = (torch.randn((A, F, T, P, 2), generator=g, device="cuda") * 8).round_().clamp_(-127, 127).to(torch.int8)
+    if args.workload.startswith("spectrometer"):
+        xf = torch.empty((A, F, T, P), dtype=torch.complex64, device="cuda")
+        yc = torch.empty((A, F * R, T // R, P), dtype=torch.complex64, device="cuda")
+        ws = torch.empty(int(lib.blade_channelize_workspace_size(A, F, T, P, R)), dtype=torch.uint8, device="cuda")
+        out = torch.empty((A, F * R, T // (R * I), 1), dtype=torch.float32, device="cuda")
+        for _ in range(args.launches):
+            _lib.call("blade_cast", _lib.CI8, _lib.CF32, x.data_ptr(), xf.data_ptr(), A * F * T * P, s)
+            _lib.call("blade_channelize", xf.data_ptr(), yc.data_ptr(), ws.data_ptr(), A, F, T, P, R, s)
+            _lib.call("blade_polarize", _lib.CF32, yc.data_ptr(), yc.data_ptr(), A * F * T, s)
+            _lib.call("blade_detect", yc.data_ptr(), out.data_ptr(), A, F * R, T // R, P, I, 1, s)
+        torch.cuda.synchronize()
+        print(f"{args.workload} modules: {args.launches} launches ok")
+        return
     tau = (torch.rand((B, A), generator=g, device="cuda", dtype=torch.float64) * 2 - 1) * 5e-6
     ph = torch.empty((B, A, F, 1, P), dtype=torch.complex64, device="cuda")
     _lib.call("blade_phasor_from_delays", tau.data_ptr(), None, ph.data_ptr(), B, A, F, P, F0_HZ, DF_HZ, 0.0, 0, s)
