@@ -364,7 +364,34 @@ def spectrometer(steps, warmup):
         res["kernels"][name] = {"ms": round(ms, 4), "bytes": nbytes, "gbs": round(gbs, 1),
                                 "frac_of_hbm": round(gbs / hbm, 3)}
     res["hbm_peak_gbs"] = hbm
-    del x, xf, yc, ws, out
+    # The same block through the fused ModeH path (blade_spectrometer): CI8 in,
+    # Stokes-I out, one FP32 workspace round trip.
+    del xf, yc
+    fws = torch.empty(int(lib.blade_spectrometer_workspace_size(A, F, T, P, R)), dtype=torch.uint8, device="cuda")
+    fout = torch.empty_like(out)
+
+    def fused():
+        _lib.call("blade_spectrometer", _lib.CI8, x.data_ptr(), _lib.F32, fout.data_ptr(), fws.data_ptr(), A, F, T, P,
+                  R, I, 1, 1, sh)
+
+    for _ in range(warmup):
+        fused()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(steps):
+        fused()
+    e1.record(s)
+    torch.cuda.synchronize()
+    fms = e0.elapsed_time(e1) / steps
+    fbytes = 2 * n + 16 * n + 4 * (n // P) // I  # CI8 in, workspace out + in, Stokes-I out
+    res["fused"] = {"api": "blade_spectrometer (ModeH)", "ms_per_step": round(fms, 4),
+                    "gbs_vs_fused_min": round(fused_min / (fms * 1e-3) / 1e9, 1),
+                    "bytes": fbytes, "gbs": round(fbytes / (fms * 1e-3) / 1e9, 1),
+                    "frac_of_hbm": round(fbytes / (fms * 1e-3) / 1e9 / hbm, 3),
+                    "speedup_over_module_chain": round(total / fms, 2),
+                    "rel_l2_vs_module_chain": float((fout - out).norm() / out.norm())}
+    del x, ws, out, fws, fout
     return res
 
 

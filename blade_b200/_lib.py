@@ -46,6 +46,8 @@ _SIGNATURES = {
     "blade_beamform_f32": (_int, [_vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _int, _int, _vp]),
     "blade_channelize_workspace_size": (_u64, [_u64, _u64, _u64, _u64, _u64]),
     "blade_channelize": (_int, [_vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp]),
+    "blade_spectrometer_workspace_size": (_u64, [_u64, _u64, _u64, _u64, _u64]),
+    "blade_spectrometer": (_int, [_int, _vp, _int, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _int, _vp]),
     "blade_polarize": (_int, [_int, _vp, _vp, _u64, _vp]),
     "blade_detect": (_int, [_vp, _vp, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),
     "blade_gather": (_int, [_u64, _vp, _vp, _u64p, _u64, _u64, _u64, _vp]),

@@ -350,8 +350,10 @@ __device__ __forceinline__ void twiddle_run(float2 (&v)[16], float2 base, float2
     }
 }
 
-template <int P>
-__global__ void __launch_bounds__(512) fft256_cols_kernel(const float2* __restrict__ in, float2* __restrict__ ws,
+// CI8 = true: the input is CI8 [.., T, 2] (one 4-byte word per dual-polarisation
+// sample), cast exactly to FP32 on load (the fused spectrometer).
+template <int P, bool CI8 = false>
+__global__ void __launch_bounds__(512, 2) fft256_cols_kernel(const void* __restrict__ vin, float2* __restrict__ ws,
                                                           uint64_t batches) {
     extern __shared__ __align__(16) float2 sm[];
     float2* tile = sm;                   // [p][jc][kLd]   (16 P columns)
@@ -367,25 +369,44 @@ __global__ void __launch_bounds__(512) fft256_cols_kernel(const float2* __restri
     for (uint64_t grp = blockIdx.x; grp < batches * 16; grp += gridDim.x) {
         const uint64_t batch = grp >> 4;
         const uint32_t c0 = (uint32_t)(grp & 15u) * 16u;
-        const float2* src = in + batch * 65536ull * P;
         __syncthreads();
         // coalesced load: rows j1 of 16 columns x P (256 B per row for P = 2); all of a
         // thread's loads are issued before any shared-memory store
         constexpr uint32_t kPer = 256u * 16u / 512u;  // 8 per thread
-        if (P == 2) {
-            float4 ld[kPer];
+        if constexpr (CI8) {
+            const uint32_t* src = static_cast<const uint32_t*>(vin) + batch * 65536ull;
+            uint32_t ld[kPer];
 #pragma unroll
             for (uint32_t u = 0; u < kPer; u++) {
                 const uint32_t e = threadIdx.x + u * 512u, j1 = e >> 4, jl = e & 15u;
-                ld[u] = ldg_nc_f4(src + 2 * ((uint64_t)j1 * 256u + c0 + jl));
+                ld[u] = __ldg(src + (uint64_t)j1 * 256u + c0 + jl);
             }
 #pragma unroll
             for (uint32_t u = 0; u < kPer; u++) {
                 const uint32_t e = threadIdx.x + u * 512u, j1 = e >> 4, jl = e & 15u;
-                tile[(0 * 16 + jl) * kLd + j1] = make_float2(ld[u].x, ld[u].y);
-                tile[(1 * 16 + jl) * kLd + j1] = make_float2(ld[u].z, ld[u].w);
+                const uint32_t w = ld[u];
+                tile[(0 * 16 + jl) * kLd + j1] = make_float2((float)(int8_t)(w & 0xFFu), (float)(int8_t)((w >> 8) & 0xFFu));
+                tile[(1 * 16 + jl) * kLd + j1] = make_float2((float)(int8_t)((w >> 16) & 0xFFu), (float)(int8_t)(w >> 24));
+            }
+        } else if (P == 2) {
+            const float2* src = static_cast<const float2*>(vin) + batch * 65536ull * P;
+#pragma unroll
+            for (uint32_t h = 0; h < 2; h++) {  // two batches of four 16-byte loads in flight
+                float4 ld[kPer / 2];
+#pragma unroll
+                for (uint32_t u = 0; u < kPer / 2; u++) {
+                    const uint32_t e = threadIdx.x + (h * kPer / 2 + u) * 512u, j1 = e >> 4, jl = e & 15u;
+                    ld[u] = ldg_nc_f4(src + 2 * ((uint64_t)j1 * 256u + c0 + jl));
+                }
+#pragma unroll
+                for (uint32_t u = 0; u < kPer / 2; u++) {
+                    const uint32_t e = threadIdx.x + (h * kPer / 2 + u) * 512u, j1 = e >> 4, jl = e & 15u;
+                    tile[(0 * 16 + jl) * kLd + j1] = make_float2(ld[u].x, ld[u].y);
+                    tile[(1 * 16 + jl) * kLd + j1] = make_float2(ld[u].z, ld[u].w);
+                }
             }
         } else {
+            const float2* src = static_cast<const float2*>(vin) + batch * 65536ull * P;
             float2 ld[kPer];
 #pragma unroll
             for (uint32_t u = 0; u < kPer; u++) {
@@ -436,11 +457,35 @@ __global__ void __launch_bounds__(512) fft256_cols_kernel(const float2* __restri
     }
 }
 
+// Loads the rows (s, p, k1) of one (a, f) for all S spectra x P polarisations
+// (q = s * P + p < nq) from the workspace into shared memory: 256 contiguous values
+// per row, pairs per 16-byte load, two batches of four loads in flight per thread.
+__device__ __forceinline__ void load_rows(const float2* __restrict__ ws, float2* rows, uint64_t af, uint32_t S,
+                                          uint32_t P, uint32_t k1, uint32_t nq) {
+#pragma unroll
+    for (uint32_t h = 0; h < 2; h++) {
+        float4 ld[4];
+#pragma unroll
+        for (uint32_t u = 0; u < 4; u++) {
+            const uint32_t e = threadIdx.x + (h * 4 + u) * 512u, j2 = (e & 127u) * 2u, qq = e >> 7;
+            if (qq < nq) ld[u] = ldg_nc_f4(ws + (((af * S) * P + qq) * 256u + k1) * 256ull + j2);
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < 4; u++) {
+            const uint32_t e = threadIdx.x + (h * 4 + u) * 512u, j2 = (e & 127u) * 2u, qq = e >> 7;
+            if (qq < nq) {
+                rows[qq * kLd + j2] = make_float2(ld[u].x, ld[u].y);
+                rows[qq * kLd + j2 + 1] = make_float2(ld[u].z, ld[u].w);
+            }
+        }
+    }
+}
+
 // Row step for N = 65536: one CTA = one (a, f) and one k1, all S spectra x P
 // polarisations (S P <= 32 FFTs, 16 threads each).  X[k1 + 256 k2] goes to the
 // fftshifted channel k1 + 256 k2 + N/2 (mod N) of [A, F*N, S, P].
 template <int P>
-__global__ void __launch_bounds__(512) fft256_rows_kernel(const float2* __restrict__ ws, float2* __restrict__ out,
+__global__ void __launch_bounds__(512, 2) fft256_rows_kernel(const float2* __restrict__ ws, float2* __restrict__ out,
                                                           uint64_t AF, uint32_t S) {
     extern __shared__ __align__(16) float2 sm[];
     float2* rows = sm;                     // [q = s P + p][kLd], q < S P <= 32
@@ -454,25 +499,7 @@ __global__ void __launch_bounds__(512) fft256_rows_kernel(const float2* __restri
         const uint64_t af = grp >> 8;
         const uint32_t k1 = (uint32_t)(grp & 255u);
         __syncthreads();
-        {
-            // rows (s, p, k1) of 256 contiguous values; pairs of values per 16-byte load,
-            // all of a thread's loads issued before the shared-memory stores
-            float4 ld[8];
-#pragma unroll
-            for (uint32_t u = 0; u < 8; u++) {
-                const uint32_t e = threadIdx.x + u * 512u, j2 = (e & 127u) * 2u, qq = e >> 7;
-                if (qq < nq)
-                    ld[u] = ldg_nc_f4(ws + (((af * S) * P + qq) * 256u + k1) * 256ull + j2);
-            }
-#pragma unroll
-            for (uint32_t u = 0; u < 8; u++) {
-                const uint32_t e = threadIdx.x + u * 512u, j2 = (e & 127u) * 2u, qq = e >> 7;
-                if (qq < nq) {
-                    rows[qq * kLd + j2] = make_float2(ld[u].x, ld[u].y);
-                    rows[qq * kLd + j2 + 1] = make_float2(ld[u].z, ld[u].w);
-                }
-            }
-        }
+        load_rows(ws, rows, af, S, P, k1, nq);
         __syncthreads();
         float2 v[16];
         if (active) {
@@ -503,6 +530,83 @@ __global__ void __launch_bounds__(512) fft256_rows_kernel(const float2* __restri
             const uint32_t qq = e % nq, k2 = e / nq;
             const uint32_t kout = (k1 + 256u * k2 + 32768u) & 65535u;
             out[((af * 65536ull + kout) * S) * P + qq] = rows[qq * kLd + k2];
+        }
+    }
+}
+
+// Row step of the fused spectrometer: the row FFTs of fft256_rows_kernel, then
+// per output channel the optional circular conversion (L, R) = (X + iY, X - iY)
+// (Polarizer), the detector over windows of I spectra (Stokes-I |X|^2 + |Y|^2, or
+// (|X|^2, |Y|^2, Re X conj Y, Im X conj Y)) and the output cast, straight to
+// out[A, F*N, S/I, OP]: only the products reach HBM.
+template <int OP, typename OT>
+__global__ void __launch_bounds__(512, 2) fft256_rows_detect_kernel(const float2* __restrict__ ws, OT* __restrict__ out,
+                                                                 uint64_t AF, uint32_t S, uint32_t I, int circular) {
+    extern __shared__ __align__(16) float2 sm[];
+    constexpr uint32_t P = 2;
+    float2* rows = sm;  // [q = s P + p][kLd], q < S P <= 32
+    float2* w256 = rows + 32 * kLd;
+    for (uint32_t m = threadIdx.x; m < 256; m += blockDim.x) w256[m] = twiddle(m, 256);
+    const uint32_t t = threadIdx.x & 15u, q = threadIdx.x >> 4;
+    const uint32_t nq = S * P, U = S / I;
+    const bool active = q < nq;
+    float2* row = rows + q * kLd;
+    for (uint64_t grp = blockIdx.x; grp < AF * 256u; grp += gridDim.x) {
+        const uint64_t af = grp >> 8;
+        const uint32_t k1 = (uint32_t)(grp & 255u);
+        __syncthreads();
+        load_rows(ws, rows, af, S, P, k1, nq);
+        __syncthreads();
+        float2 v[16];
+        if (active) {
+#pragma unroll
+            for (int n1 = 0; n1 < 16; n1++) v[n1] = row[16 * n1 + t];
+            dft16(v);
+            twiddle_run(v, make_float2(1.f, 0.f), w256[t]);
+        }
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < 16; k++) row[kZ * t + k] = v[k];
+        }
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int n2 = 0; n2 < 16; n2++) v[n2] = row[kZ * n2 + t];
+            dft16(v);
+        }
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int c = 0; c < 16; c++) row[t + 16 * c] = v[c];
+        }
+        __syncthreads();
+        // one thread per (k2, u): window sum over I spectra, OP products
+        for (uint32_t e = threadIdx.x; e < 256u * U; e += blockDim.x) {
+            const uint32_t u = e % U, k2 = e / U;
+            float acc[OP];
+#pragma unroll
+            for (int o = 0; o < OP; o++) acc[o] = 0.f;
+            for (uint32_t s = u * I; s < (u + 1) * I; s++) {
+                float2 x = rows[(s * 2 + 0) * kLd + k2], y = rows[(s * 2 + 1) * kLd + k2];
+                if (circular) {
+                    const float2 l = make_float2(x.x - y.y, x.y + y.x), r = make_float2(x.x + y.y, x.y - y.x);
+                    x = l;
+                    y = r;
+                }
+                if constexpr (OP == 1) {
+                    acc[0] += x.x * x.x + x.y * x.y + y.x * y.x + y.y * y.y;
+                } else {
+                    acc[0] += x.x * x.x + x.y * x.y;
+                    acc[1] += y.x * y.x + y.y * y.y;
+                    acc[2] += x.x * y.x + x.y * y.y;  // Re x conj(y)
+                    acc[3] += x.y * y.x - x.x * y.y;  // Im x conj(y)
+                }
+            }
+            const uint32_t kout = (k1 + 256u * k2 + 32768u) & 65535u;
+            OT* dst = out + ((af * 65536ull + kout) * U + u) * OP;
+#pragma unroll
+            for (int o = 0; o < OP; o++) dst[o] = (OT)acc[o];
         }
     }
 }
@@ -605,12 +709,12 @@ extern "C" int blade_channelize(const void* in, void* out, void* workspace, uint
         if (P == 2) {
             if ((rc = prepare_smem(fft256_cols_kernel<2>, sm1))) return rc;
             if ((rc = prepare_smem(fft256_rows_kernel<2>, sm2))) return rc;
-            fft256_cols_kernel<2><<<(unsigned)(g1 < cap ? g1 : cap), 512, sm1, s>>>(src, ws, batches);
+            fft256_cols_kernel<2><<<(unsigned)(g1 < cap ? g1 : cap), 512, sm1, s>>>(in, ws, batches);
             fft256_rows_kernel<2><<<(unsigned)(g2 < cap ? g2 : cap), 512, sm2, s>>>(ws, dst, A * F, (uint32_t)S);
         } else {
             if ((rc = prepare_smem(fft256_cols_kernel<1>, sm1))) return rc;
             if ((rc = prepare_smem(fft256_rows_kernel<1>, sm2))) return rc;
-            fft256_cols_kernel<1><<<(unsigned)(g1 < cap ? g1 : cap), 512, sm1, s>>>(src, ws, batches);
+            fft256_cols_kernel<1><<<(unsigned)(g1 < cap ? g1 : cap), 512, sm1, s>>>(in, ws, batches);
             fft256_rows_kernel<1><<<(unsigned)(g2 < cap ? g2 : cap), 512, sm2, s>>>(ws, dst, A * F, (uint32_t)S);
         }
         return check_launch("blade_channelize");
@@ -640,4 +744,76 @@ extern "C" int blade_channelize(const void* in, void* out, void* workspace, uint
             ws, dst, (uint32_t)A, (uint32_t)F, (uint32_t)T, (uint32_t)N1, (uint32_t)N2, (uint32_t)SB2, p2);
     }
     return check_launch("blade_channelize");
+}
+
+// ---- fused spectrometer (Cast -> Channelizer -> Polarizer -> Detector -> Cast) ----
+
+extern "C" uint64_t blade_spectrometer_workspace_size(uint64_t A, uint64_t F, uint64_t T, uint64_t P, uint64_t rate) {
+    if (P != 2 || rate != 65536 || T % rate) return 0;
+    return A * F * T * P * sizeof(float2);
+}
+
+extern "C" int blade_spectrometer(int in_type, const void* in, int out_type, void* out, void* workspace, uint64_t A,
+                                  uint64_t F, uint64_t T, uint64_t P, uint64_t rate, uint64_t integration,
+                                  uint64_t out_pols, int circular, blade_stream_t stream) {
+    using namespace bb;
+    if (in_type != BLADE_CI8 && in_type != BLADE_CF32)
+        return set_error(BLADE_ERROR, "blade_spectrometer: input must be CI8 or CF32");
+    if (out_type != BLADE_F32 && out_type != BLADE_F16)
+        return set_error(BLADE_ERROR, "blade_spectrometer: output must be F32 or F16");
+    if (P != 2) return set_error(BLADE_ERROR, "blade_spectrometer: the polarizer needs two polarizations (P = %llu)",
+                                 (unsigned long long)P);
+    if (rate != 65536)
+        return set_error(BLADE_ERROR, "blade_spectrometer: the fused path runs rate 65536 (256 x 256); use the "
+                         "module chain for rate %llu", (unsigned long long)rate);
+    if (T % rate != 0)
+        return set_error(BLADE_ERROR, "blade_spectrometer: the number of time samples (%llu) should be divisible by "
+                         "the channelizer rate (%llu)", (unsigned long long)T, (unsigned long long)rate);
+    const uint64_t S = T / rate;
+    if (S > 16) return set_error(BLADE_ERROR, "blade_spectrometer: at most 16 spectra per block (T <= 2^20)");
+    if (integration == 0)
+        return set_error(BLADE_ERROR, "blade_spectrometer: integration size (%llu) should be more than zero",
+                         (unsigned long long)integration);
+    if (S % integration != 0)
+        return set_error(BLADE_ERROR, "blade_spectrometer: the number of spectra (%llu) should be divisible by the "
+                         "integration size (%llu)", (unsigned long long)S, (unsigned long long)integration);
+    if (out_pols != 1 && out_pols != 4)
+        return set_error(BLADE_ERROR, "blade_spectrometer: number of output polarizations (%llu) not supported",
+                         (unsigned long long)out_pols);
+    if (A * F == 0) return BLADE_SUCCESS;
+    if (!in || !out || !workspace) return set_error(BLADE_ERROR, "blade_spectrometer: null buffer");
+    if (!aligned16(in) || !aligned16(workspace) || (reinterpret_cast<uintptr_t>(out) & 3))
+        return set_error(BLADE_ERROR, "blade_spectrometer: input and workspace must be 16-byte aligned");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    float2* ws = static_cast<float2*>(workspace);
+    const uint64_t batches = A * F * S;
+    const size_t sm1 = (16 * 2 * kLd + 512) * sizeof(float2), sm2 = (32 * kLd + 256) * sizeof(float2);
+    const uint64_t cap = (uint64_t)sm_count() * 2;
+    const uint64_t g1 = batches * 16, g2 = A * F * 256;
+    const unsigned grid1 = (unsigned)(g1 < cap ? g1 : cap), grid2 = (unsigned)(g2 < cap ? g2 : cap);
+    int rc;
+    if (in_type == BLADE_CI8) {
+        if ((rc = prepare_smem(fft256_cols_kernel<2, true>, sm1))) return rc;
+        fft256_cols_kernel<2, true><<<grid1, 512, sm1, s>>>(in, ws, batches);
+    } else {
+        if ((rc = prepare_smem(fft256_cols_kernel<2, false>, sm1))) return rc;
+        fft256_cols_kernel<2, false><<<grid1, 512, sm1, s>>>(in, ws, batches);
+    }
+    if ((rc = check_launch("blade_spectrometer"))) return rc;
+    const uint32_t S32 = (uint32_t)S, I32 = (uint32_t)integration;
+#define BB_SPEC_ROWS(OPN, OTY)                                                                              \
+    do {                                                                                                    \
+        if ((rc = prepare_smem(fft256_rows_detect_kernel<OPN, OTY>, sm2))) return rc;                       \
+        fft256_rows_detect_kernel<OPN, OTY><<<grid2, 512, sm2, s>>>(ws, static_cast<OTY*>(out), A * F, S32, \
+                                                                    I32, circular ? 1 : 0);                 \
+    } while (0)
+    if (out_type == BLADE_F32) {
+        if (out_pols == 1) BB_SPEC_ROWS(1, float);
+        else BB_SPEC_ROWS(4, float);
+    } else {
+        if (out_pols == 1) BB_SPEC_ROWS(1, __half);
+        else BB_SPEC_ROWS(4, __half);
+    }
+#undef BB_SPEC_ROWS
+    return check_launch("blade_spectrometer");
 }

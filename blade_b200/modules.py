@@ -703,6 +703,86 @@ class BeamformDetect(Module):
         return result.success
 
 
+class ModeH(Module):
+    """Bundles::Generic::ModeH<IT, OT> (include/blade/bundles/generic/mode_h.hh:55-106,
+    Python binding python/blade/ext_modeh.cc:21-45):
+    Cast -> Channelizer -> Polarizer -> Detector -> output Cast, fused into two
+    kernels (blade_spectrometer) so that only the input, an FP32 workspace and the
+    detector products touch device memory.  rate defaults to the number of time
+    samples as in ModeH; the fused path runs rate 65536 (256 x 256) with up to 16
+    spectra per block (the module chain covers every other rate)."""
+
+    taint = Taint.CONSUMER | Taint.PRODUCER
+
+    @dataclass
+    class config:
+        input_shape: Sequence[int]
+        output_shape: Sequence[int]
+        polarizer_convert_to_circular: bool
+        detector_integration_size: int
+        detector_number_of_output_polarizations: int
+        cast_block_size: int = 512
+        polarizer_block_size: int = 512
+        channelizer_block_size: int = 512
+        detector_block_size: int = 512
+        rate: int = 0  # not in the reference: 0 = the number of time samples, as ModeH
+
+    @dataclass
+    class input:
+        buffer: object
+
+    def __init__(self, config, input, stream=None, it="ci8", ot="f32"):
+        super().__init__()
+        self.config, self._input = config, input
+        buf = as_vector(input.buffer)
+        if buf.dtype not in ("ci8", "cf32") or ot not in ("f32", "f16"):
+            _fail("ModeH takes CI8 or CF32 voltages and produces F32 or F16.")
+        A, F, T, P = buf.shape
+        if tuple(config.input_shape) != tuple(buf.shape):
+            _fail(f"Expected input buffer size ({tuple(config.input_shape)}) mismatch with actual size "
+                  f"({tuple(buf.shape)}).")
+        R = int(config.rate) or T
+        I, OP = int(config.detector_integration_size), int(config.detector_number_of_output_polarizations)
+        if P != 2:
+            _fail(f"The polarizer needs two polarizations (P = {P}).")
+        if R <= 0 or T % R != 0:
+            _fail(f"The number of time samples ({T}) should be divisible by the channelizer rate ({R}).")
+        if I <= 0 or (T // R) % I != 0:
+            _fail(f"The number of spectra ({T // R}) should be divisible by the integration size ({I}).")
+        if OP not in (1, 4):
+            _fail(f"Number of output polarizations ({OP}) not supported.")
+        lib = _lib.load()
+        n = int(lib.blade_spectrometer_workspace_size(A, F, T, P, R))
+        if n == 0:
+            _fail(f"The fused spectrometer runs rate 65536; use the module chain for rate {R}.")
+        self._rate, self._ot = R, ot
+        self._workspace = torch.empty(n, dtype=torch.uint8, device="cuda")
+        self._shape = (A, F * R, T // (R * I), OP)
+        if tuple(config.output_shape) != self._shape:
+            _fail(f"Expected output buffer size ({tuple(config.output_shape)}) mismatch with actual size "
+                  f"({self._shape}).")
+        self._output = self._alloc(self._shape, ot)
+
+    def get_config(self):
+        return self.config
+
+    def get_input_buffer(self):
+        return self._input.buffer
+
+    def get_output(self):
+        return self._output
+
+    def process(self, step=0, stream=None):
+        buf, out = as_vector(self._input.buffer), _out(self._output)
+        A, F, T, P = buf.shape
+        c = self.config
+        _lib.call("blade_spectrometer", type_code(buf.dtype), buf.data_ptr(), type_code(self._ot), out.data_ptr(),
+                  self._workspace.data_ptr(), A, F, T, P, self._rate, int(c.detector_integration_size),
+                  int(c.detector_number_of_output_polarizations), 1 if c.polarizer_convert_to_circular else 0,
+                  _stream_handle(stream))
+        return result.success
+
+
 # Registry used by blade_b200.module(): (name, telescope) -> (class, {(it, ot)}).
 _CAST_PAIRS = {("i8", "i8"), ("i8", "f32"), ("f16", "f32"), ("f16", "f16"), ("f32", "i32"), ("f32", "f16"),
                ("f32", "f32"), ("ci8", "cf32"), ("ci8", "cf16"), ("ci8", "ci8"), ("cf32", "cf16"),
@@ -724,4 +804,5 @@ REGISTRY = {
     ("phasor", "generic"): (Phasor, {("f64", "cf32")}),
     ("beamform_detect", "ata"): (BeamformDetect, {("ci8", "f32"), ("cf32", "f32")}),
     ("beamform_detect", "generic"): (BeamformDetect, {("ci8", "f32"), ("cf32", "f32")}),
+    ("modeh", "generic"): (ModeH, {("ci8", "f32"), ("ci8", "f16"), ("cf32", "f32"), ("cf32", "f16")}),
 }

@@ -116,6 +116,26 @@ BLADE_API int blade_channelize(const void* in, void* out, void* workspace,
                      blade_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Fused spectrometer: Cast -> Channelizer(rate) -> Polarizer -> Detector ->
+ * output Cast in two kernels, [A,F,T,2] CI8 or CF32 in, [A,F*rate,T/(rate*I),
+ * out_pols] F32 or F16 out; only the input, an FP32 workspace of
+ * blade_spectrometer_workspace_size() bytes and the detector products touch HBM.
+ * circular != 0 converts (X, Y) to (X + iY, X - iY) before the detector (the
+ * Polarizer's XY -> LR), else the detector sees (X, Y).  rate must be 65536
+ * (split 256 x 256), T a multiple of it with at most 16 spectra, I dividing the
+ * spectra, out_pols 1 or 4 (as blade_detect).  Same results as the module chain
+ * blade_cast, blade_channelize, blade_polarize, blade_detect.
+ * Replaces Bundles::Generic::ModeH<IT,OT> (include/blade/bundles/generic/
+ * mode_h.hh:55-106), whose channelizer runs rate == T only.
+ * ------------------------------------------------------------------------- */
+BLADE_API uint64_t blade_spectrometer_workspace_size(uint64_t A, uint64_t F, uint64_t T,
+                                           uint64_t P, uint64_t rate);
+BLADE_API int blade_spectrometer(int in_type, const void* in, int out_type, void* out,
+                       void* workspace, uint64_t A, uint64_t F, uint64_t T, uint64_t P,
+                       uint64_t rate, uint64_t integration, uint64_t out_pols,
+                       int circular, blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Polarizer: per dual-pol sample (X, Y) -> (X + iY, X - iY); in may equal out.
  * type in {BLADE_CF32, BLADE_CF16}; n_samples = A*F*T (P must be 2).
  * Replaces Modules::Polarizer::process, src/modules/polarizer/base.cc:61-68

@@ -96,3 +96,24 @@ def test_channelize_workspace_size():
     lib = _lib.load()
     assert lib.blade_channelize_workspace_size(1, 64, 1 << 20, 2, 4096) == 0
     assert lib.blade_channelize_workspace_size(1, 64, 1 << 20, 2, 65536) == 64 * (1 << 20) * 2 * 8
+
+
+def test_spectrometer_validation():
+    lib = _lib.load()
+    R = 65536
+    assert lib.blade_spectrometer_workspace_size(1, 64, 1 << 20, 2, R) == 64 * (1 << 20) * 2 * 8
+    assert lib.blade_spectrometer_workspace_size(1, 64, 1 << 20, 2, 4096) == 0
+    bad = [
+        ((_lib.CF16, _lib.F32, 1, 1, 2 * R, 2, R, 1, 1), "input"),
+        ((_lib.CI8, _lib.CF32, 1, 1, 2 * R, 2, R, 1, 1), "output"),
+        ((_lib.CI8, _lib.F32, 1, 1, 2 * R, 1, R, 1, 1), "two"),
+        ((_lib.CI8, _lib.F32, 1, 1, 2 * 4096, 2, 4096, 1, 1), "65536"),
+        ((_lib.CI8, _lib.F32, 1, 1, 3 * R + 1, 2, R, 1, 1), "divisible"),
+        ((_lib.CI8, _lib.F32, 1, 1, 32 * R, 2, R, 1, 1), "16 spectra"),
+        ((_lib.CI8, _lib.F32, 1, 1, 2 * R, 2, R, 0, 1), "zero"),
+        ((_lib.CI8, _lib.F32, 1, 1, 6 * R, 2, R, 4, 1), "integration"),
+        ((_lib.CI8, _lib.F32, 1, 1, 2 * R, 2, R, 1, 2), "polarizations"),
+    ]
+    for (it, ot, A, F, T, P, rate, I, OP), word in bad:
+        st, msg = _err("blade_spectrometer", it, None, ot, None, None, A, F, T, P, rate, I, OP, 0, None)
+        assert st == _lib.ERROR and word in msg, (word, msg)
