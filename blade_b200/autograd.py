@@ -34,10 +34,10 @@ def _adjoint(x: torch.Tensor, w: torch.Tensor):
     if tuple(w.shape) != (B, A, F, 1, P):
         raise RuntimeError(f"weights shape {tuple(w.shape)} does not match voltages {tuple(x.shape)}")
     grad = torch.empty_like(w)
-    loss = torch.empty(F * P, dtype=torch.float64, device=x.device)
+    loss = torch.empty(1, dtype=torch.float64, device=x.device)
     _lib.call("blade_beamform_detect_adjoint", x.data_ptr(), w.data_ptr(), grad.data_ptr(), loss.data_ptr(), B, A, F,
               T, P, torch.cuda.current_stream().cuda_stream)
-    return loss.sum(), grad
+    return loss[0], grad
 
 
 class StokesLoss(torch.autograd.Function):

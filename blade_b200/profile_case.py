@@ -5,7 +5,9 @@
 Workloads: ata-small (A=20 F=96 T=256 B=8 rate 1 I=4), ata-production
 (A=28 F=192 T=8192 B=16 rate 4 I=4), dense-64x64 (A=64 F=256 T=8192 B=64 rate 1
 I=8), spectrometer (A=1 F=64 T=2^20, rate 65536, I=8, no beamformer) and
-spectrometer-small (the same with F=16, for full profiler captures).  Paths: tc
+spectrometer-small (the same with F=16, for full profiler captures), calibration
+(A=28 F=192 T=2048 B=1, CF32 voltages; path adjoint: the Stokes loss and its
+gradient).  Paths: tc
 (phasor split + tensor-core chain), f32 (fused FP32 chain), modules (Cast ->
 Beamformer -> Channelizer -> Detector, one launch each; for the spectrometer
 Cast -> Channelizer -> Polarizer -> Detector).
@@ -27,13 +29,14 @@ WORKLOADS = {
     "dense-64x64": dict(A=64, F=256, T=8192, B=64, R=1, I=8),
     "spectrometer": dict(A=1, F=64, T=1 << 20, B=0, R=65536, I=8),
     "spectrometer-small": dict(A=1, F=16, T=1 << 20, B=0, R=65536, I=8),
+    "calibration": dict(A=28, F=192, T=2048, B=1, R=1, I=1),
 }
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="ata-production", choices=sorted(WORKLOADS))
-    ap.add_argument("--path", default="tc", choices=["tc", "f32", "modules"])
+    ap.add_argument("--path", default="tc", choices=["tc", "f32", "modules", "adjoint"])
     ap.add_argument("--launches", type=int, default=4)
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
@@ -42,6 +45,19 @@ def main():
     s = torch.cuda.current_stream().cuda_stream
     g = torch.Generator(device="cuda").manual_seed(7)
     x = (torch.randn((A, F, T, P, 2), generator=g, device="cuda") * 8).round_().clamp_(-127, 127).to(torch.int8)
+    if args.path == "adjoint":
+        xc = torch.complex(torch.randn((A, F, T, P), generator=g, device="cuda"),
+                           torch.randn((A, F, T, P), generator=g, device="cuda"))
+        wc = torch.polar(torch.ones((B, A, F, 1, P), device="cuda"),
+                         torch.rand((B, A, F, 1, P), generator=g, device="cuda") * 6.283185307)
+        grad = torch.empty_like(wc)
+        loss = torch.empty(1, dtype=torch.float64, device="cuda")
+        for _ in range(args.launches):
+            _lib.call("blade_beamform_detect_adjoint", xc.data_ptr(), wc.data_ptr(), grad.data_ptr(), loss.data_ptr(),
+                      B, A, F, T, P, s)
+        torch.cuda.synchronize()
+        print(f"{args.workload} adjoint: {args.launches} launches ok")
+        return
     if args.workload.startswith("spectrometer"):
         xf = torch.empty((A, F, T, P), dtype=torch.complex64, device="cuda")
         yc = torch.empty((A, F * R, T // R, P), dtype=torch.complex64, device="cuda")

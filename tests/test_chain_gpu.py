@@ -115,9 +115,25 @@ def test_adjoint_gradient_vs_fp64(cuda, A, F, T, B):
     w = (rng.standard_normal((B, A, F, 1, 2)) + 1j * rng.standard_normal((B, A, F, 1, 2))) / np.sqrt(A)
     xd, wd = c64(x), c64(w)
     gd = torch.zeros((B, A, F, 1, 2), dtype=torch.complex64, device="cuda")
-    ld = torch.zeros(F * 2, dtype=torch.float64, device="cuda")
+    ld = torch.zeros(1, dtype=torch.float64, device="cuda")
     call("blade_beamform_detect_adjoint", ptr(xd), ptr(wd), ptr(gd), ptr(ld), B, A, F, T, 2, stream())
     x32, w32 = x.astype(np.complex64), w.astype(np.complex64)
     g_ref = O.stokes_loss_grad(x32, w32)
     assert rel_l2(host(gd), g_ref) < TOL
-    assert abs(host(ld).sum() - O.stokes_loss(x32, w32)) / abs(O.stokes_loss(x32, w32)) < TOL
+    assert abs(host(ld)[0] - O.stokes_loss(x32, w32)) / abs(O.stokes_loss(x32, w32)) < TOL
+
+
+@pytest.mark.parametrize("A,F,T,B,P", [(9, 4, 640, 2, 1), (40, 2, 256, 40, 2)])
+def test_adjoint_general_path_vs_fp64(cuda, A, F, T, B, P):
+    # one polarisation, and B x A above the main path's pair limit, take the
+    # one-CTA-per-(f, p) kernel; same gradient and scalar loss
+    rng = np.random.default_rng(A * B + P)
+    x = (rng.standard_normal((A, F, T, P)) + 1j * rng.standard_normal((A, F, T, P))).astype(np.complex64)
+    w = ((rng.standard_normal((B, A, F, 1, P)) + 1j * rng.standard_normal((B, A, F, 1, P))) / np.sqrt(A)).astype(
+        np.complex64)
+    gd = torch.zeros((B, A, F, 1, P), dtype=torch.complex64, device="cuda")
+    ld = torch.zeros(1, dtype=torch.float64, device="cuda")
+    xd, wd = c64(x), c64(w)  # keep the device copies alive until the kernels have run
+    call("blade_beamform_detect_adjoint", ptr(xd), ptr(wd), ptr(gd), ptr(ld), B, A, F, T, P, stream())
+    assert rel_l2(host(gd), O.stokes_loss_grad(x, w)) < TOL
+    assert abs(host(ld)[0] - O.stokes_loss(x, w)) / abs(O.stokes_loss(x, w)) < TOL
