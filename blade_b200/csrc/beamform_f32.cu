@@ -283,6 +283,34 @@ __global__ void __launch_bounds__(256) incoherent_kernel(const float2* __restric
     }
 }
 
+// Small blocks (the tiled kernel would leave SMs idle): one thread per
+// (beam, channel, sample) and both polarisations, antennas in order; the CTA's
+// phasors are the same for all its threads and its voltages come from L2 (every
+// beam re-reads them).  Same arithmetic as the tiled kernel per output.
+template <int P>
+__global__ void __launch_bounds__(256) bf32_small_kernel(const float2* __restrict__ in,
+                                                         const float2* __restrict__ phasors, float2* __restrict__ out,
+                                                         uint32_t A, uint32_t F, uint32_t T) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, f = blockIdx.y, b = blockIdx.z;
+    if (t >= T) return;
+    float2 acc[P];
+#pragma unroll
+    for (int p = 0; p < P; p++) acc[p] = make_float2(0.f, 0.f);
+    const float2* x = in + ((uint64_t)f * T + t) * P;
+    const float2* w = phasors + ((uint64_t)b * A * F + f) * P;
+    for (uint32_t a = 0; a < A; a++) {
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            const float2 xv = __ldg(x + (uint64_t)a * F * T * P + p), wv = __ldg(w + (uint64_t)a * F * P + p);
+            acc[p].x = fmaf(xv.x, wv.x, fmaf(-xv.y, wv.y, acc[p].x));
+            acc[p].y = fmaf(xv.x, wv.y, fmaf(xv.y, wv.x, acc[p].y));
+        }
+    }
+    float2* o = out + (((uint64_t)b * F + f) * T + t) * P;
+#pragma unroll
+    for (int p = 0; p < P; p++) o[p] = acc[p];
+}
+
 template <int P, int TG, int IN, int R>
 void launch_bf(const void* in, const float2* ph, void* out, uint64_t B, uint64_t A, uint64_t F, uint64_t T,
                uint64_t integ, cudaStream_t s) {
@@ -326,8 +354,20 @@ extern "C" int blade_beamform_f32(const void* in, const void* phasors, void* out
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const float2* ph = static_cast<const float2*>(phasors);
     const int tg = pick_tg(B);
-    if (P == 2) dispatch_tg<2, IN_CF32, 0>(tg, in, ph, out, B, A, F, T, 1, s);
-    else dispatch_tg<1, IN_CF32, 0>(tg, in, ph, out, B, A, F, T, 1, s);
+    const uint64_t tiles = ceil_div(T, (uint64_t)tg * 4) * F * ceil_div(B, (uint64_t)(256 / tg) * 4);
+    if (tiles < 2ull * sm_count() && B <= 65535) {
+        const dim3 grid((unsigned)ceil_div(T, 256), (unsigned)F, (unsigned)B);
+        if (P == 2)
+            bf32_small_kernel<2><<<grid, 256, 0, s>>>(static_cast<const float2*>(in), ph, static_cast<float2*>(out),
+                                                      (uint32_t)A, (uint32_t)F, (uint32_t)T);
+        else
+            bf32_small_kernel<1><<<grid, 256, 0, s>>>(static_cast<const float2*>(in), ph, static_cast<float2*>(out),
+                                                      (uint32_t)A, (uint32_t)F, (uint32_t)T);
+    } else if (P == 2) {
+        dispatch_tg<2, IN_CF32, 0>(tg, in, ph, out, B, A, F, T, 1, s);
+    } else {
+        dispatch_tg<1, IN_CF32, 0>(tg, in, ph, out, B, A, F, T, 1, s);
+    }
     if (incoherent) {
         if (P == 2)
             incoherent_kernel<2><<<grid_for(F * T, 256), 256, 0, s>>>(static_cast<const float2*>(in), ph,

@@ -122,6 +122,9 @@ extern "C" int blade_detect(const void* in, void* out, uint64_t A, uint64_t F, u
     float* dst = static_cast<float*>(out);
     if (integration <= 1024) {
         uint32_t wpc = (uint32_t)(kChunk / integration);
+        // small inputs: shorter chunks so that at least two CTAs per SM have work
+        const uint64_t fill = ceil_div(n_windows, (uint64_t)sm_count() * 2);
+        if (fill < wpc) wpc = (uint32_t)(fill > 0 ? fill : 1);
         uint64_t chunks = ceil_div(n_windows, wpc);
         unsigned grid = (unsigned)(chunks < (uint64_t)sm_count() * 8 ? chunks : (uint64_t)sm_count() * 8);
         if (out_pols == 1)
