@@ -445,10 +445,15 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
     // issue of tcgen05.mma holds its thread for about the MMA's duration, so one
     // issuer's waits and commits overlap the other's MMAs.
     const uint32_t nis = (pair && ((AS / 2) & 1u) == 0 && (nacc & 1u) == 0) ? 2u : 1u;
+    // Split operand build (R = 4, two issuers, two-tile raw stages): converter warps
+    // 0-3 build the even tiles of the CTA's range (the first tile of each raw stage,
+    // issuer 0's) and warps 4-7 the odd ones, so the two halves run independently
+    // and each operand pair has four producers.
+    const bool split = R == 4 && nis == 2 && g.raw_tiles == 2;
 
     if (threadIdx.x == 0) {
         for (uint32_t i = 0; i < AS; i++) {
-            mbar_init(&a_full[i], kConvWarps);
+            mbar_init(&a_full[i], split ? kConvWarps / 2 : kConvWarps);
             mbar_init(&a_empty[i], 1);
         }
         for (uint32_t i = 0; i < RS; i++) {
@@ -644,7 +649,10 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
             float* obase = g.out + ((uint64_t)f * R + k) * g.U + u;
             constexpr int CH = 16 / kEpiGroups;  // beams per TMEM load (16 or 8)
             for (uint32_t bc = hw * nbh; bc < (hw + 1) * nbh; bc += CH) {
-                float pw[CH];
+                // Two beams per packed FP32x2 instruction (each lane of the pair rounds
+                // exactly as the scalar add / multiply / FMA would).
+                float2 pw2[CH / 2];
+                float(&pw)[CH] = *reinterpret_cast<float(*)[CH]>(pw2);
                 if (g.stacked) {
                     // per polarisation: (hi + lo) re, (hi + lo) im
 #pragma unroll
@@ -659,10 +667,12 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
                         tmem_ld(pa + 3 * NB, li);
                         tmem_ld_wait();
 #pragma unroll
-                        for (int j = 0; j < CH; j++) {
-                            const float a = __uint_as_float(hr[j]) + __uint_as_float(lr[j]);
-                            const float b = __uint_as_float(hi[j]) + __uint_as_float(li[j]);
-                            pw[j] = fmaf(a, a, fmaf(b, b, pw[j]));
+                        for (int j = 0; j < CH / 2; j++) {
+                            const float2 a = __fadd2_rn(make_float2(__uint_as_float(hr[2 * j]), __uint_as_float(hr[2 * j + 1])),
+                                                        make_float2(__uint_as_float(lr[2 * j]), __uint_as_float(lr[2 * j + 1])));
+                            const float2 b = __fadd2_rn(make_float2(__uint_as_float(hi[2 * j]), __uint_as_float(hi[2 * j + 1])),
+                                                        make_float2(__uint_as_float(li[2 * j]), __uint_as_float(li[2 * j + 1])));
+                            pw2[j] = __ffma2_rn(a, a, __ffma2_rn(b, b, pw2[j]));
                         }
                     }
                 } else {
@@ -673,10 +683,12 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
                     tmem_ld(lane_addr + 3 * NB + bc, i1);
                     tmem_ld_wait();
 #pragma unroll
-                    for (int j = 0; j < CH; j++) {
-                        const float a0 = __uint_as_float(r0[j]), b0 = __uint_as_float(i0[j]);
-                        const float a1 = __uint_as_float(r1[j]), b1 = __uint_as_float(i1[j]);
-                        pw[j] = fmaf(a0, a0, fmaf(b0, b0, fmaf(a1, a1, b1 * b1)));
+                    for (int j = 0; j < CH / 2; j++) {
+                        const float2 a0 = make_float2(__uint_as_float(r0[2 * j]), __uint_as_float(r0[2 * j + 1]));
+                        const float2 b0 = make_float2(__uint_as_float(i0[2 * j]), __uint_as_float(i0[2 * j + 1]));
+                        const float2 a1 = make_float2(__uint_as_float(r1[2 * j]), __uint_as_float(r1[2 * j + 1]));
+                        const float2 b1 = make_float2(__uint_as_float(i1[2 * j]), __uint_as_float(i1[2 * j + 1]));
+                        pw2[j] = __ffma2_rn(a0, a0, __ffma2_rn(b0, b0, __ffma2_rn(a1, a1, __fmul2_rn(b1, b1))));
                     }
                 }
                 uint32_t first;
@@ -698,6 +710,42 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
     } else if (warp < 2 + kEpiWarps + kConvWarps) {
         // ---------------- operand build ----------------
         const uint32_t ct = threadIdx.x - (2 + kEpiWarps) * 32;  // 0 .. 32 kConvWarps - 1
+        if constexpr (R == 4) {
+            if (split) {
+                // Group grp takes local tiles grp, grp + 2, ...: tile `grp` of every raw
+                // stage (512 bytes into each 1 KB antenna row) and operand pair 2 grp,
+                // 2 grp + 4, ... (the pairs issuer grp consumes).  The CTA's range is a
+                // whole number of two-tile stages, so both groups see every stage once.
+                constexpr uint32_t kGroup = kConvWarps / 2;
+                constexpr uint32_t kMaxTk = kMaxKA / 4 / kGroup;
+                const uint32_t cw = ct >> 5, grp = cw / kGroup, gw = cw % kGroup;
+                const uint32_t ntk = KA / 4 / kGroup;
+                R4Task tk[kMaxTk];
+#pragma unroll
+                for (uint32_t i = 0; i < kMaxTk; i++) tk[i] = r4_task(gw + i * kGroup, lane, g.A, KA, g.raw_row);
+                uint32_t rs = 0, rph = 0, as = 2 * grp, aph = 0;
+                for (uint64_t L = L0 + grp; L < L1; L += 2) {
+                    if (!mbar_wait(&r_full[rs], rph, abort, kWaitBudget)) { record_abort(abort, 11); break; }
+                    if (!mbar_wait(&a_empty[as + 1], aph ^ 1, abort, kWaitBudget)) { record_abort(abort, 8); break; }
+                    const uint8_t* raw = r_smem + (size_t)rs * g.raw_bytes + grp * (kM * 4u);
+                    uint8_t* op0 = a_smem + (size_t)as * op_bytes;
+                    uint8_t* op1 = op0 + op_bytes;
+#pragma unroll
+                    for (uint32_t i = 0; i < kMaxTk; i++)
+                        if (i < ntk) r4_pair_task(raw, g.raw_row, op0, op1, tk[i]);
+                    fence_proxy_async_smem();
+                    __syncwarp();
+                    if (lane == 0) {
+                        mbar_arrive(&a_full[as + 1]);
+                        mbar_arrive(&r_empty[rs]);
+                    }
+                    as += 4;
+                    if (as >= AS) { as -= AS; aph ^= 1; }
+                    if (++rs == RS) { rs = 0; rph ^= 1; }
+                }
+            }
+        }
+        if (!(R == 4 && split)) {
         // R = 4 pair mode: this warp's warp-tasks (KA / 4 of them over kConvWarps warps),
         // addresses fixed for the kernel
         constexpr uint32_t kMaxT4 = kMaxKA / 4 / kConvWarps;
@@ -754,6 +802,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
                 if (lane == 0) mbar_arrive(&r_empty[rs]);
                 if (++rs == RS) { rs = 0; rph ^= 1; }
             }
+        }
         }
     }
 
