@@ -783,6 +783,147 @@ class ModeH(Module):
         return result.success
 
 
+class ModeB(Module):
+    """Bundles::ATA::ModeB<IT, OT> (include/blade/bundles/ata/mode_b.hh:17-225, Python
+    binding python/blade/ext_modeb.cc:20-114): Cast -> Channelizer (pre-beamformer,
+    rate R) -> Polarizer -> Phasor -> Beamformer::ATA -> [Detector] on one stream.
+
+    The geometric half of the phasor stage (ERFA astrometry from antenna positions,
+    beam coordinates, julian date and DUT1, src/modules/phasor/ata.cc:9-173) is not
+    part of this library: the input carries either the phasors themselves
+    (``phasors``, CF32 [B, A, F*R, 1, P]) or per-beam delays (``delays``, F64 [B, A]
+    seconds), which the Phasor stage turns into phasors with the ``phasor_*``
+    frequency fields and ``phasor_antenna_calibrations`` (ata.cc:176-208).  The
+    position and coordinate fields are accepted and unused.
+
+    With the detector enabled the incoherent beam is square-rooted, as the bundle
+    configures it (mode_b.hh:146-147).  When the chain is Beamformer -> Detector
+    alone (rate 1, no circular conversion, no incoherent beam, Stokes-I), it runs
+    as one fused launch (tensor cores for CI8 input, FP32 CUDA cores for CF32);
+    every other configuration runs the module kernels in order."""
+
+    taint = Taint.CONSUMER | Taint.PRODUCER
+
+    @dataclass
+    class config:
+        input_shape: Sequence[int]
+        output_shape: Sequence[int]
+        pre_beamformer_channelizer_rate: int = 1
+        pre_beamformer_polarizer_convert_to_circular: bool = False
+        phasor_observation_frequency_hz: float = 0.0
+        phasor_channel_bandwidth_hz: float = 0.0
+        phasor_total_bandwidth_hz: float = 0.0
+        phasor_frequency_start_index: int = 0
+        phasor_reference_antenna_index: int = 0
+        phasor_array_reference_position: object = None
+        phasor_boresight_coordinate: object = None
+        phasor_antenna_positions: object = None
+        phasor_antenna_calibrations: object = None  # CF64 [A, F*R, 1, P], None = unit
+        phasor_beam_coordinates: object = None
+        beamformer_incoherent_beam: bool = False
+        detector_enable: bool = False
+        detector_integration_size: int = 1
+        detector_number_of_output_polarizations: int = 1
+        cast_block_size: int = 512
+        channelizer_block_size: int = 512
+        phasor_block_size: int = 512
+        beamformer_block_size: int = 512
+        polarizer_block_size: int = 512
+        detector_block_size: int = 512
+
+    @dataclass
+    class input:
+        buffer: object
+        phasors: object = None
+        delays: object = None
+
+    def __init__(self, config, input, stream=None, it="ci8", ot="f32"):
+        super().__init__()
+        self.config, self._input = config, input
+        c = config
+        buf = as_vector(input.buffer)
+        if buf.dtype != it or it not in ("ci8", "cf32"):
+            _fail(f"ModeB takes CI8 or CF32 voltages (buffer is {buf.dtype}, expected {it}).")
+        if ot not in ("f32", "cf32") or (ot == "f32") != bool(c.detector_enable):
+            _fail("ModeB produces F32 with the detector enabled and CF32 without it.")
+        if tuple(c.input_shape) != tuple(buf.shape):
+            _fail(f"Expected input buffer size ({tuple(c.input_shape)}) mismatch with actual size "
+                  f"({tuple(buf.shape)}).")
+        A, F, T, P = buf.shape
+        R = int(c.pre_beamformer_channelizer_rate)
+        if (input.phasors is None) == (input.delays is None):
+            _fail("ModeB needs exactly one of input.phasors (CF32 [B, A, F*R, 1, P]) or input.delays (F64 [B, A]).")
+        self._stages = []
+        self._phasor = None
+        if input.delays is not None:
+            d = as_vector(input.delays)
+            if len(d.shape) != 2:
+                _fail("ModeB delays must be an F64 delay_tensor [B, A].")
+            self._phasor = Phasor(Phasor.config(
+                number_of_beams=d.shape[0], number_of_antennas=A, number_of_frequency_channels=F * R,
+                number_of_polarizations=P, observation_frequency_hz=c.phasor_observation_frequency_hz,
+                channel_bandwidth_hz=c.phasor_channel_bandwidth_hz, total_bandwidth_hz=c.phasor_total_bandwidth_hz,
+                frequency_start_index=c.phasor_frequency_start_index,
+                antenna_calibrations=c.phasor_antenna_calibrations, block_size=c.phasor_block_size),
+                Phasor.input(delays=input.delays))
+            phasors = self._phasor.get_phasors()
+        else:
+            phasors = input.phasors
+        ph = as_vector(phasors)
+        B = ph.shape[0]
+        if tuple(ph.shape) != (B, A, F * R, 1, P):
+            _fail(f"Phasor shape {tuple(ph.shape)} does not match the channelized voltages ({B}, {A}, {F * R}, 1, {P}).")
+        I, OP = int(c.detector_integration_size), int(c.detector_number_of_output_polarizations)
+        self.fused = (c.detector_enable and R == 1 and not c.pre_beamformer_polarizer_convert_to_circular
+                      and not c.beamformer_incoherent_beam and OP == 1 and P == 2 and I > 0 and T % I == 0)
+        if self.fused:
+            last = BeamformDetect(BeamformDetect.config(rate=1, integration_size=I, number_of_output_polarizations=1),
+                                  BeamformDetect.input(buffer=input.buffer, phasors=phasors), it=it, ot="f32")
+            self._stages.append(last)
+        else:
+            cast = Cast(Cast.config(c.cast_block_size), Cast.input(input.buffer), it=it, ot="cf32")
+            chan = Channelizer(Channelizer.config(R, c.channelizer_block_size), Channelizer.input(cast.get_output()))
+            polz = Polarizer(Polarizer.config(pol.xy, pol.lr if c.pre_beamformer_polarizer_convert_to_circular
+                                              else pol.xy, c.polarizer_block_size),
+                             Polarizer.input(chan.get_output()))
+            bf = BeamformerATA(BeamformerATA.config(bool(c.beamformer_incoherent_beam), bool(c.detector_enable),
+                                                    c.beamformer_block_size),
+                               BeamformerATA.input(polz.get_output(), phasors))
+            self._stages += [cast, chan, polz, bf]
+            last = bf
+            if c.detector_enable:
+                last = Detector(Detector.config(I, OP, c.detector_block_size), Detector.input(bf.get_output()))
+                self._stages.append(last)
+        self._last = last
+        out_shape = tuple(as_vector(last.get_output()).shape)
+        if tuple(c.output_shape) != out_shape:
+            _fail(f"Expected output buffer size ({tuple(c.output_shape)}) mismatch with actual size ({out_shape}).")
+
+    def _set_slot(self, index: int) -> None:
+        super()._set_slot(index)
+        for m in ([self._phasor] if self._phasor is not None else []) + self._stages:
+            m._set_slot(index)
+
+    def get_config(self):
+        return self.config
+
+    def get_input_buffer(self):
+        return self._input.buffer
+
+    def get_phasors(self):
+        return self._phasor.get_phasors() if self._phasor is not None else self._input.phasors
+
+    def get_output(self):
+        return self._last.get_output()
+
+    def process(self, step=0, stream=None):
+        for m in ([self._phasor] if self._phasor is not None else []) + self._stages:
+            res = m.process(step, stream)
+            if res != result.success:
+                return res
+        return result.success
+
+
 # Registry used by blade_b200.module(): (name, telescope) -> (class, {(it, ot)}).
 _CAST_PAIRS = {("i8", "i8"), ("i8", "f32"), ("f16", "f32"), ("f16", "f16"), ("f32", "i32"), ("f32", "f16"),
                ("f32", "f32"), ("ci8", "cf32"), ("ci8", "cf16"), ("ci8", "ci8"), ("cf32", "cf16"),
@@ -805,4 +946,5 @@ REGISTRY = {
     ("beamform_detect", "ata"): (BeamformDetect, {("ci8", "f32"), ("cf32", "f32")}),
     ("beamform_detect", "generic"): (BeamformDetect, {("ci8", "f32"), ("cf32", "f32")}),
     ("modeh", "generic"): (ModeH, {("ci8", "f32"), ("ci8", "f16"), ("cf32", "f32"), ("cf32", "f16")}),
+    ("modeb", "ata"): (ModeB, {("ci8", "cf32"), ("cf32", "cf32"), ("ci8", "f32"), ("cf32", "f32")}),
 }

@@ -325,7 +325,7 @@ def module(name, config, input, it=None, ot=None, telescope=K.generic):
         default_in, default_out = "cf32", "f32"
     if _name == "phasor":
         default_in, default_out = "f64", "cf32"
-    if _name in ("beamform_detect", "modeh"):
+    if _name in ("beamform_detect", "modeh", "modeb"):
         default_in, default_out = "ci8", "f32"
     for label, v in (("input", it), ("output", ot)):
         if v is not None and not isinstance(v, Constant):

@@ -242,6 +242,26 @@ def spectrometer(x_ci8: np.ndarray, rate: int, integration: int, polarizer: bool
     return detect(y, integration, npols)
 
 
+def mode_b(x: np.ndarray, phasors: np.ndarray, rate: int, circular: bool = False, incoherent: bool = False,
+           detector: bool = True, integration: int = 1, npols: int = 1) -> np.ndarray:
+    """Cast -> Channelizer(rate) -> Polarizer -> Beamformer::ATA -> [Detector].
+
+    The ATA ModeB chain of ``include/blade/bundles/ata/mode_b.hh:99-199`` (the
+    phasors are per channelized channel, [B, A, F*rate, 1, P]; the incoherent beam
+    is square-rooted when the detector is enabled, ``mode_b.hh:146-147``) and the
+    Stokes-I reduction of its test oracle ``tests/bundles/ata/mode_b.py:377-390``.
+    ``x`` is CI8 ([..., 2] int8) or complex.
+    """
+    x = ci8_to_complex(x) if np.asarray(x).dtype == np.int8 else np.asarray(x, dtype=np.complex128)
+    y = channelize(x, rate)
+    if circular:
+        y = polarize(y)
+    z = beamform(y, phasors, incoherent=incoherent, incoherent_sqrt=detector)
+    if not detector:
+        return z
+    return detect(z, integration, npols)
+
+
 # --------------------------------------------------------------------------- #
 # Adjoint of beamform + Stokes-I detect (no reference counterpart)
 # --------------------------------------------------------------------------- #

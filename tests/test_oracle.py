@@ -156,3 +156,33 @@ def test_chain_rate4_equals_stepwise():
     y = O.beamform_channelize_detect(x, w, 4, 2)
     step = O.detect(O.channelize(O.beamform(O.ci8_to_complex(x), w), 4), 2, 1)
     np.testing.assert_allclose(y, step, rtol=1e-12)
+
+
+def test_mode_b_matches_reference_test_loops():
+    # tests/bundles/ata/mode_b.py:377-390: per beam, the antenna sum of input x phasors,
+    # then |x|^2 + |y|^2 per sample (rate 1, integration 1, no polarizer).
+    rng = np.random.default_rng(13)
+    A, F, T, P, B = 4, 3, 8, 2, 2
+    x = crand(rng, (A, F, T, P))
+    w = crand(rng, (B, A, F, 1, P))
+    out = np.zeros((B, F, T, 1))
+    for ib in range(B):
+        phased = (x.astype(np.complex128) * w[ib][..., :].astype(np.complex128)).sum(axis=0)
+        for ic in range(F):
+            for it in range(T):
+                xx, yy = phased[ic, it, 0], phased[ic, it, 1]
+                out[ib, ic, it, 0] = xx.real * xx.real + xx.imag * xx.imag + yy.real * yy.real + yy.imag * yy.imag
+    np.testing.assert_allclose(O.mode_b(x, w, 1), out, rtol=1e-12)
+
+
+def test_mode_b_incoherent_beam_is_square_rooted_before_the_detector():
+    rng = np.random.default_rng(14)
+    x = crand(rng, (3, 2, 16, 2))
+    w = crand(rng, (2, 3, 4, 1, 2))
+    out = O.mode_b(x, w, 2, circular=True, incoherent=True, detector=True, integration=2)
+    y = O.polarize(O.channelize(x, 2))
+    inc = (np.abs(y * w[0]) ** 2).sum(axis=0)                # [F*R, T/R, P]
+    ref = (inc.reshape(4, 4, 2, 2)).sum(axis=(2, 3))         # sqrt then |.|^2 gives the sum back
+    np.testing.assert_allclose(out[2, :, :, 0], ref, rtol=1e-12)
+    stepwise = O.detect(O.beamform(y, w), 2, 1)
+    np.testing.assert_allclose(out[:2], stepwise, rtol=1e-12)
