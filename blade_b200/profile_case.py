@@ -10,7 +10,7 @@ spectrometer-small (the same with F=16, for full profiler captures), calibration
 gradient).  Paths: tc
 (phasor split + tensor-core chain), f32 (fused FP32 chain), modules (Cast ->
 Beamformer -> Channelizer -> Detector, one launch each; for the spectrometer
-Cast -> Channelizer -> Polarizer -> Detector).
+Cast -> Channelizer -> Polarizer -> Detector; path fused: blade_spectrometer).
 Inputs are seeded synthetic CI8 voltages and phasors, created on the device.
 """
 
@@ -36,7 +36,7 @@ WORKLOADS = {
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="ata-production", choices=sorted(WORKLOADS))
-    ap.add_argument("--path", default="tc", choices=["tc", "f32", "modules", "adjoint"])
+    ap.add_argument("--path", default="tc", choices=["tc", "f32", "modules", "adjoint", "fused"])
     ap.add_argument("--launches", type=int, default=4)
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
@@ -57,6 +57,15 @@ def main():
                       B, A, F, T, P, s)
         torch.cuda.synchronize()
         print(f"{args.workload} adjoint: {args.launches} launches ok")
+        return
+    if args.workload.startswith("spectrometer") and args.path == "fused":
+        out = torch.empty((A, F * R, T // (R * I), 1), dtype=torch.float32, device="cuda")
+        ws = torch.empty(int(lib.blade_spectrometer_workspace_size(A, F, T, P, R)), dtype=torch.uint8, device="cuda")
+        for _ in range(args.launches):
+            _lib.call("blade_spectrometer", _lib.CI8, x.data_ptr(), _lib.F32, out.data_ptr(), ws.data_ptr(), A, F, T,
+                      P, R, I, 1, 1, s)
+        torch.cuda.synchronize()
+        print(f"{args.workload} fused: {args.launches} launches ok")
         return
     if args.workload.startswith("spectrometer"):
         xf = torch.empty((A, F, T, P), dtype=torch.complex64, device="cuda")
