@@ -18,6 +18,7 @@
 #include <tuple>
 #include <vector>
 
+#include "blade/bundles.hh"
 #include "blade/modules.hh"
 
 namespace Blade {
@@ -55,7 +56,11 @@ class Pipeline {
                  const typename Block::Input& input) {
         if (_commited) throw Error(Result::ERROR, "Can't connect new module after Pipeline is commited.");
         module = std::make_shared<Block>(config, input, _streams[0]);
-        addModule(module);
+        if constexpr (std::is_base_of<Bundle, Block>::value) {
+            for (auto& m : module->getModules()) addModule(m);  // a bundle runs as its modules, in order
+        } else {
+            addModule(module);
+        }
     }
 
     void addModule(const std::shared_ptr<Module>& module) {
