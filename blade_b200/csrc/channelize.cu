@@ -366,21 +366,31 @@ __global__ void __launch_bounds__(512, 2) fft256_cols_kernel(const void* __restr
     const uint32_t t = threadIdx.x & 15u, jc = (threadIdx.x >> 4) & 15u, p = threadIdx.x >> 8;
     const bool active = p < (uint32_t)P;
     float2* col = tile + (p * 16 + jc) * kLd;
+    constexpr uint32_t kPer = 256u * 16u / 512u;  // words loaded per thread per group
+    // CI8: the next group's words are loaded into registers while this group's FFTs
+    // run (8 registers), so the loads of consecutive groups overlap the arithmetic.
+    uint32_t nxt[kPer];
+    auto load_ci8 = [&](uint64_t g, uint32_t (&w)[kPer]) {
+        const uint32_t* src = static_cast<const uint32_t*>(vin) + (g >> 4) * 65536ull + (uint32_t)(g & 15u) * 16u;
+#pragma unroll
+        for (uint32_t u = 0; u < kPer; u++) {
+            const uint32_t e = threadIdx.x + u * 512u;
+            w[u] = __ldg(src + (uint64_t)(e >> 4) * 256u + (e & 15u));
+        }
+    };
+    if constexpr (CI8)
+        if (blockIdx.x < batches * 16) load_ci8(blockIdx.x, nxt);
     for (uint64_t grp = blockIdx.x; grp < batches * 16; grp += gridDim.x) {
         const uint64_t batch = grp >> 4;
         const uint32_t c0 = (uint32_t)(grp & 15u) * 16u;
         __syncthreads();
         // coalesced load: rows j1 of 16 columns x P (256 B per row for P = 2); all of a
         // thread's loads are issued before any shared-memory store
-        constexpr uint32_t kPer = 256u * 16u / 512u;  // 8 per thread
         if constexpr (CI8) {
-            const uint32_t* src = static_cast<const uint32_t*>(vin) + batch * 65536ull;
             uint32_t ld[kPer];
 #pragma unroll
-            for (uint32_t u = 0; u < kPer; u++) {
-                const uint32_t e = threadIdx.x + u * 512u, j1 = e >> 4, jl = e & 15u;
-                ld[u] = __ldg(src + (uint64_t)j1 * 256u + c0 + jl);
-            }
+            for (uint32_t u = 0; u < kPer; u++) ld[u] = nxt[u];
+            if (grp + gridDim.x < batches * 16) load_ci8(grp + gridDim.x, nxt);
 #pragma unroll
             for (uint32_t u = 0; u < kPer; u++) {
                 const uint32_t e = threadIdx.x + u * 512u, j1 = e >> 4, jl = e & 15u;
@@ -459,26 +469,20 @@ __global__ void __launch_bounds__(512, 2) fft256_cols_kernel(const void* __restr
 
 // Loads the rows (s, p, k1) of one (a, f) for all S spectra x P polarisations
 // (q = s * P + p < nq) from the workspace into shared memory: 256 contiguous values
-// per row, pairs per 16-byte load, two batches of four loads in flight per thread.
+// per row.
 __device__ __forceinline__ void load_rows(const float2* __restrict__ ws, float2* rows, uint64_t af, uint32_t S,
                                           uint32_t P, uint32_t k1, uint32_t nq) {
-#pragma unroll
-    for (uint32_t h = 0; h < 2; h++) {
-        float4 ld[4];
-#pragma unroll
-        for (uint32_t u = 0; u < 4; u++) {
-            const uint32_t e = threadIdx.x + (h * 4 + u) * 512u, j2 = (e & 127u) * 2u, qq = e >> 7;
-            if (qq < nq) ld[u] = ldg_nc_f4(ws + (((af * S) * P + qq) * 256u + k1) * 256ull + j2);
-        }
-#pragma unroll
-        for (uint32_t u = 0; u < 4; u++) {
-            const uint32_t e = threadIdx.x + (h * 4 + u) * 512u, j2 = (e & 127u) * 2u, qq = e >> 7;
-            if (qq < nq) {
-                rows[qq * kLd + j2] = make_float2(ld[u].x, ld[u].y);
-                rows[qq * kLd + j2 + 1] = make_float2(ld[u].z, ld[u].w);
-            }
-        }
+    // Asynchronous 8-byte copies straight into shared memory: all of a group's loads
+    // are in flight at once without holding registers (rows are 273 float2 apart, so
+    // 8 bytes is the widest aligned copy); consecutive threads take consecutive j2.
+    const uint32_t n = nq * 256u;
+    for (uint32_t e = threadIdx.x; e < n; e += blockDim.x) {
+        const uint32_t qq = e >> 8, j2 = e & 255u;
+        const float2* src = ws + (((af * S) * P + qq) * 256u + k1) * 256ull + j2;
+        const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(rows + qq * kLd + j2));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // Row step for N = 65536: one CTA = one (a, f) and one k1, all S spectra x P
