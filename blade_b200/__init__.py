@@ -23,8 +23,8 @@ from .constants import *  # noqa: F401,F403  (bl.cf32, bl.ata, bl.beamformer, bl
 from .constants import Constant, Taint, pol, result
 from .memory import Duet, Vector, array_tensor, delay_tensor, phasor_tensor, tensor
 from .memory import copy as _mem_copy
-from .modules import (BeamformDetect, BeamformerATA, Cast, Channelizer, Detector, Duplicate, Gather, ModeB, ModeH,
-                      Module, Permutation, Phasor, Polarizer)
+from .modules import (BeamformDetect, BeamformerATA, BeamformerMeerKAT, Cast, Channelizer, Detector, Duplicate,
+                      Gather, ModeB, ModeH, Module, Permutation, Phasor, Polarizer)
 from .runtime import Pipeline, Runner, module, runner
 
 __version__ = "1.0.0"

@@ -44,6 +44,7 @@ _SIGNATURES = {
     "blade_cast": (_int, [_int, _int, _vp, _vp, _u64, _vp]),
     "blade_phasor_from_delays": (_int, [_vp, _vp, _vp, _u64, _u64, _u64, _u64, _dbl, _dbl, _dbl, _u64, _vp]),
     "blade_beamform_f32": (_int, [_vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _int, _int, _vp]),
+    "blade_beamform_meerkat_f32": (_int, [_vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _int, _vp]),
     "blade_channelize_workspace_size": (_u64, [_u64, _u64, _u64, _u64, _u64]),
     "blade_channelize": (_int, [_vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp]),
     "blade_spectrometer_workspace_size": (_u64, [_u64, _u64, _u64, _u64, _u64]),

@@ -94,6 +94,42 @@ class ATA : public Module {
     const Input input;
     SlotOutput<ArrayTensor<Device::CUDA, OT>> out;
 };
+
+// include/blade/modules/beamformer/meerkat.hh, src/modules/beamformer/meerkat.cc:8-39:
+// one weight per (beam, antenna), the first B*A values of the phasor tensor, for
+// every channel and polarisation; the incoherent beam is sized but zero (the
+// reference kernel never writes it).
+template <typename IT, typename OT>
+class MeerKAT : public Module {
+   public:
+    using Config = typename ATA<IT, OT>::Config;
+    using Input = typename ATA<IT, OT>::Input;
+
+    MeerKAT(const Config& config, const Input& input, const Stream& = nullptr)
+        : config(config), input(input), out(outShape(config, input)) {}
+
+    const ArrayTensor<Device::CUDA, OT>& getOutputBuffer() const { return out.get(); }
+    Taint getTaint() const override { return Taint::CONSUMER | Taint::PRODUCER; }
+    std::string name() const override { return "Beamformer"; }
+    void setSlot(U64 i) override { out.set(i); }
+    Result process(const U64&, const Stream& stream = nullptr) override {
+        const auto& s = input.buf.shape();
+        return FromABI(blade_beamform_meerkat_f32(input.buf.data(), input.phasors.data(), out.get().data(),
+                                                  input.phasors.shape().numberOfBeams(), s.numberOfAspects(),
+                                                  s.numberOfFrequencyChannels(), s.numberOfTimeSamples(),
+                                                  s.numberOfPolarizations(), config.enableIncoherentBeam, stream));
+    }
+
+   private:
+    static ArrayShape outShape(const Config& c, const Input& in) {
+        const auto& s = in.buf.shape();
+        return ArrayShape({in.phasors.shape().numberOfBeams() + (c.enableIncoherentBeam ? 1 : 0),
+                           s.numberOfFrequencyChannels(), s.numberOfTimeSamples(), s.numberOfPolarizations()});
+    }
+    const Config config;
+    const Input input;
+    SlotOutput<ArrayTensor<Device::CUDA, OT>> out;
+};
 }  // namespace Beamformer
 
 // ---------------------------------------------------------------- Channelizer

@@ -28,6 +28,15 @@ namespace {
 
 enum { IN_CF32 = 0, IN_CI8 = 1 };
 
+// Phasor element strides (float2 units) of beam, antenna, channel and
+// polarisation: [B, A, F, 1, P] for ATA, (A, 1, 0, 0) for MeerKAT's [B, A] weights
+// shared by every channel and polarisation.
+struct PhLayout {
+    uint64_t sb, sa, sf, sp;
+};
+
+inline PhLayout ata_layout(uint64_t A, uint64_t F, uint64_t P) { return PhLayout{A * F * P, F * P, P, 1}; }
+
 __device__ __forceinline__ void cmac(float2& acc, float2 x, float2 w) {
     acc.x = fmaf(x.x, w.x, acc.x);
     acc.x = fmaf(-x.y, w.y, acc.x);
@@ -43,7 +52,7 @@ __device__ __forceinline__ float pw(float2 a) { return a.x * a.x + a.y * a.y; }
 template <int P, int TG, int IN, int R>
 __global__ void __launch_bounds__(256, 2) bf32_kernel(const void* __restrict__ vin, const float2* __restrict__ phasors,
                                                    void* __restrict__ vout, uint32_t B, uint32_t A, uint32_t F,
-                                                   uint32_t T, uint32_t integ) {
+                                                   uint32_t T, uint32_t integ, const PhLayout ph) {
     constexpr int BGN = 256 / TG;
     constexpr int BT = BGN * 4;
     constexpr int TT = TG * 4;
@@ -104,7 +113,8 @@ __global__ void __launch_bounds__(256, 2) bf32_kernel(const void* __restrict__ v
             if (e < AC * BT * P) {
                 const int p = e % P, j = (e / P) % BT, al = e / (P * BT);
                 const uint32_t a = a0 + al, b = b0 + j;
-                if (a < A && b < B) wr[m] = __ldg(phasors + ((uint64_t)(b * (uint64_t)A + a) * F + f) * P + p);
+                if (a < A && b < B)
+                    wr[m] = __ldg(phasors + b * ph.sb + a * ph.sa + (uint64_t)f * ph.sf + (uint64_t)p * ph.sp);
             }
         }
     };
@@ -290,18 +300,18 @@ __global__ void __launch_bounds__(256) incoherent_kernel(const float2* __restric
 template <int P>
 __global__ void __launch_bounds__(256) bf32_small_kernel(const float2* __restrict__ in,
                                                          const float2* __restrict__ phasors, float2* __restrict__ out,
-                                                         uint32_t A, uint32_t F, uint32_t T) {
+                                                         uint32_t A, uint32_t F, uint32_t T, const PhLayout ph) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, f = blockIdx.y, b = blockIdx.z;
     if (t >= T) return;
     float2 acc[P];
 #pragma unroll
     for (int p = 0; p < P; p++) acc[p] = make_float2(0.f, 0.f);
     const float2* x = in + ((uint64_t)f * T + t) * P;
-    const float2* w = phasors + ((uint64_t)b * A * F + f) * P;
+    const float2* w = phasors + b * ph.sb + (uint64_t)f * ph.sf;
     for (uint32_t a = 0; a < A; a++) {
 #pragma unroll
         for (int p = 0; p < P; p++) {
-            const float2 xv = __ldg(x + (uint64_t)a * F * T * P + p), wv = __ldg(w + (uint64_t)a * F * P + p);
+            const float2 xv = __ldg(x + (uint64_t)a * F * T * P + p), wv = __ldg(w + a * ph.sa + p * ph.sp);
             acc[p].x = fmaf(xv.x, wv.x, fmaf(-xv.y, wv.y, acc[p].x));
             acc[p].y = fmaf(xv.x, wv.y, fmaf(xv.y, wv.x, acc[p].y));
         }
@@ -313,28 +323,66 @@ __global__ void __launch_bounds__(256) bf32_small_kernel(const float2* __restric
 
 template <int P, int TG, int IN, int R>
 void launch_bf(const void* in, const float2* ph, void* out, uint64_t B, uint64_t A, uint64_t F, uint64_t T,
-               uint64_t integ, cudaStream_t s) {
+               uint64_t integ, cudaStream_t s, const PhLayout& lay) {
     constexpr int TT = TG * 4, BT = (256 / TG) * 4;
     dim3 grid((unsigned)ceil_div(T, TT), (unsigned)F, (unsigned)ceil_div(B, BT));
     bf32_kernel<P, TG, IN, R><<<grid, 256, 0, s>>>(in, ph, out, (uint32_t)B, (uint32_t)A, (uint32_t)F, (uint32_t)T,
-                                                   (uint32_t)integ);
+                                                   (uint32_t)integ, lay);
 }
 
 int pick_tg(uint64_t B) { return B <= 4 ? 256 : B <= 8 ? 128 : B <= 16 ? 64 : 32; }
 
 template <int P, int IN, int R>
 void dispatch_tg(int tg, const void* in, const float2* ph, void* out, uint64_t B, uint64_t A, uint64_t F, uint64_t T,
-                 uint64_t integ, cudaStream_t s) {
+                 uint64_t integ, cudaStream_t s, const PhLayout& lay) {
     switch (tg) {
-        case 256: launch_bf<P, 256, IN, R>(in, ph, out, B, A, F, T, integ, s); break;
-        case 128: launch_bf<P, 128, IN, R>(in, ph, out, B, A, F, T, integ, s); break;
-        case 64: launch_bf<P, 64, IN, R>(in, ph, out, B, A, F, T, integ, s); break;
-        default: launch_bf<P, 32, IN, R>(in, ph, out, B, A, F, T, integ, s); break;
+        case 256: launch_bf<P, 256, IN, R>(in, ph, out, B, A, F, T, integ, s, lay); break;
+        case 128: launch_bf<P, 128, IN, R>(in, ph, out, B, A, F, T, integ, s, lay); break;
+        case 64: launch_bf<P, 64, IN, R>(in, ph, out, B, A, F, T, integ, s, lay); break;
+        default: launch_bf<P, 32, IN, R>(in, ph, out, B, A, F, T, integ, s, lay); break;
     }
 }
 
 bool dims_ok(uint64_t B, uint64_t A, uint64_t F, uint64_t T) {
     return B < (1u << 31) && A < (1u << 31) && F <= 65535 && T < (1u << 31) && ceil_div(B, 4) <= 65535;
+}
+
+}  // namespace
+}  // namespace bb
+
+namespace bb {
+namespace {
+
+// Beams 0..B-1 of the plain FP32 beamformer for a phasor layout (no incoherent beam).
+int beamform_f32_beams(const char* who, const void* in, const float2* ph, void* out, uint64_t B, uint64_t A,
+                       uint64_t F, uint64_t T, uint64_t P, const PhLayout& lay, cudaStream_t s) {
+    if (B == 0) return BLADE_SUCCESS;
+    const int tg = pick_tg(B);
+    const uint64_t tiles = ceil_div(T, (uint64_t)tg * 4) * F * ceil_div(B, (uint64_t)(256 / tg) * 4);
+    if (tiles < 2ull * sm_count() && B <= 65535) {
+        const dim3 grid((unsigned)ceil_div(T, 256), (unsigned)F, (unsigned)B);
+        if (P == 2)
+            bf32_small_kernel<2><<<grid, 256, 0, s>>>(static_cast<const float2*>(in), ph, static_cast<float2*>(out),
+                                                      (uint32_t)A, (uint32_t)F, (uint32_t)T, lay);
+        else
+            bf32_small_kernel<1><<<grid, 256, 0, s>>>(static_cast<const float2*>(in), ph, static_cast<float2*>(out),
+                                                      (uint32_t)A, (uint32_t)F, (uint32_t)T, lay);
+    } else if (P == 2) {
+        dispatch_tg<2, IN_CF32, 0>(tg, in, ph, out, B, A, F, T, 1, s, lay);
+    } else {
+        dispatch_tg<1, IN_CF32, 0>(tg, in, ph, out, B, A, F, T, 1, s, lay);
+    }
+    return check_launch(who);
+}
+
+int check_f32_args(const char* who, const void* in, const void* phasors, void* out, uint64_t B, uint64_t A,
+                   uint64_t F, uint64_t T, uint64_t P) {
+    if (P != 1 && P != 2) return set_error(BLADE_ERROR, "%s: P must be 1 or 2", who);
+    if (!in || !phasors || !out) return set_error(BLADE_ERROR, "%s: null buffer", who);
+    if (!dims_ok(B, A, F, T)) return set_error(BLADE_ERROR, "%s: dimensions out of range", who);
+    if (P == 2 && (!aligned16(in) || !aligned16(out)))
+        return set_error(BLADE_ERROR, "%s: dual-pol buffers must be 16-byte aligned", who);
+    return BLADE_SUCCESS;
 }
 
 }  // namespace
@@ -346,28 +394,12 @@ extern "C" int blade_beamform_f32(const void* in, const void* phasors, void* out
     if (P != 1 && P != 2) return set_error(BLADE_ERROR, "blade_beamform_f32: P must be 1 or 2");
     if (B == 0 && !incoherent) return BLADE_SUCCESS;
     if (A == 0 || F == 0 || T == 0) return BLADE_SUCCESS;
-    if (!in || !phasors || !out) return set_error(BLADE_ERROR, "blade_beamform_f32: null buffer");
-    if (!dims_ok(B, A, F, T)) return set_error(BLADE_ERROR, "blade_beamform_f32: dimensions out of range");
+    if (int rc = check_f32_args("blade_beamform_f32", in, phasors, out, B, A, F, T, P)) return rc;
     if (incoherent && B == 0) return set_error(BLADE_ERROR, "blade_beamform_f32: incoherent beam needs beam 0");
-    if (P == 2 && (!aligned16(in) || !aligned16(out)))
-        return set_error(BLADE_ERROR, "blade_beamform_f32: dual-pol buffers must be 16-byte aligned");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const float2* ph = static_cast<const float2*>(phasors);
-    const int tg = pick_tg(B);
-    const uint64_t tiles = ceil_div(T, (uint64_t)tg * 4) * F * ceil_div(B, (uint64_t)(256 / tg) * 4);
-    if (tiles < 2ull * sm_count() && B <= 65535) {
-        const dim3 grid((unsigned)ceil_div(T, 256), (unsigned)F, (unsigned)B);
-        if (P == 2)
-            bf32_small_kernel<2><<<grid, 256, 0, s>>>(static_cast<const float2*>(in), ph, static_cast<float2*>(out),
-                                                      (uint32_t)A, (uint32_t)F, (uint32_t)T);
-        else
-            bf32_small_kernel<1><<<grid, 256, 0, s>>>(static_cast<const float2*>(in), ph, static_cast<float2*>(out),
-                                                      (uint32_t)A, (uint32_t)F, (uint32_t)T);
-    } else if (P == 2) {
-        dispatch_tg<2, IN_CF32, 0>(tg, in, ph, out, B, A, F, T, 1, s);
-    } else {
-        dispatch_tg<1, IN_CF32, 0>(tg, in, ph, out, B, A, F, T, 1, s);
-    }
+    if (int rc = beamform_f32_beams("blade_beamform_f32", in, ph, out, B, A, F, T, P, ata_layout(A, F, P), s))
+        return rc;
     if (incoherent) {
         if (P == 2)
             incoherent_kernel<2><<<grid_for(F * T, 256), 256, 0, s>>>(static_cast<const float2*>(in), ph,
@@ -381,6 +413,25 @@ extern "C" int blade_beamform_f32(const void* in, const void* phasors, void* out
                                                                      incoherent_sqrt);
     }
     return check_launch("blade_beamform_f32");
+}
+
+extern "C" int blade_beamform_meerkat_f32(const void* in, const void* phasors, void* out, uint64_t B, uint64_t A,
+                                          uint64_t F, uint64_t T, uint64_t P, int incoherent, blade_stream_t stream) {
+    using namespace bb;
+    if (B == 0 && !incoherent) return BLADE_SUCCESS;
+    if (A == 0 || F == 0 || T == 0) return BLADE_SUCCESS;
+    if (int rc = check_f32_args("blade_beamform_meerkat_f32", in, phasors, out, B, A, F, T, P)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (int rc = beamform_f32_beams("blade_beamform_meerkat_f32", in, static_cast<const float2*>(phasors), out, B, A,
+                                    F, T, P, PhLayout{A, 1, 0, 0}, s))
+        return rc;
+    if (incoherent) {
+        // the reference sizes the incoherent beam but its MeerKAT kernel never writes it
+        const cudaError_t e =
+            cudaMemsetAsync(static_cast<float2*>(out) + B * F * T * P, 0, F * T * P * sizeof(float2), s);
+        if (e != cudaSuccess) return check_cuda(e, "blade_beamform_meerkat_f32");
+    }
+    return check_launch("blade_beamform_meerkat_f32");
 }
 
 extern "C" int blade_beamform_detect_f32(int in_type, const void* in, const void* phasors, void* out, uint64_t B,
@@ -420,14 +471,15 @@ extern "C" int blade_beamform_detect_f32(int in_type, const void* in, const void
         return set_error(BLADE_ERROR, "blade_beamform_detect_f32: CI8 input must be 4-byte aligned");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const float2* ph = static_cast<const float2*>(phasors);
+    const PhLayout lay = ata_layout(A, F, 2);
     if (in_type == BLADE_CI8) {
-        if (rate == 1) dispatch_tg<2, IN_CI8, 1>(tg, in, ph, out, B, A, F, T, integration, s);
-        else if (rate == 2) dispatch_tg<2, IN_CI8, 2>(tg, in, ph, out, B, A, F, T, integration, s);
-        else dispatch_tg<2, IN_CI8, 4>(tg, in, ph, out, B, A, F, T, integration, s);
+        if (rate == 1) dispatch_tg<2, IN_CI8, 1>(tg, in, ph, out, B, A, F, T, integration, s, lay);
+        else if (rate == 2) dispatch_tg<2, IN_CI8, 2>(tg, in, ph, out, B, A, F, T, integration, s, lay);
+        else dispatch_tg<2, IN_CI8, 4>(tg, in, ph, out, B, A, F, T, integration, s, lay);
     } else {
-        if (rate == 1) dispatch_tg<2, IN_CF32, 1>(tg, in, ph, out, B, A, F, T, integration, s);
-        else if (rate == 2) dispatch_tg<2, IN_CF32, 2>(tg, in, ph, out, B, A, F, T, integration, s);
-        else dispatch_tg<2, IN_CF32, 4>(tg, in, ph, out, B, A, F, T, integration, s);
+        if (rate == 1) dispatch_tg<2, IN_CF32, 1>(tg, in, ph, out, B, A, F, T, integration, s, lay);
+        else if (rate == 2) dispatch_tg<2, IN_CF32, 2>(tg, in, ph, out, B, A, F, T, integration, s, lay);
+        else dispatch_tg<2, IN_CF32, 4>(tg, in, ph, out, B, A, F, T, integration, s, lay);
     }
     return check_launch("blade_beamform_detect_f32");
 }

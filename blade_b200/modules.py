@@ -199,6 +199,23 @@ class BeamformerATA(Module):
         return result.success
 
 
+class BeamformerMeerKAT(BeamformerATA):
+    """Modules::Beamformer::MeerKAT<CF32, CF32> (include/blade/modules/beamformer/meerkat.hh,
+    src/modules/beamformer/meerkat.cc:8-39, kernel beamformer.cu:81-117): one weight
+    per (beam, antenna) for every channel and polarisation, read as the first B*A
+    values of the [B, A, F, 1, P] phasor tensor (as the reference kernel indexes it).
+    The incoherent beam is sized as in the reference, which never writes it; here it
+    is zero."""
+
+    def process(self, step=0, stream=None):
+        buf, ph, out = as_vector(self._input.buffer), as_vector(self._input.phasors), _out(self._output)
+        A, F, T, P = buf.shape
+        B = ph.shape[0]
+        _lib.call("blade_beamform_meerkat_f32", buf.data_ptr(), ph.data_ptr(), out.data_ptr(), B, A, F, T, P,
+                  int(self.config.enable_incoherent_beam), _stream_handle(stream))
+        return result.success
+
+
 # =============================================================================
 # Channelizer
 # =============================================================================
@@ -935,6 +952,7 @@ _CAST_PAIRS = {("i8", "i8"), ("i8", "f32"), ("f16", "f32"), ("f16", "f16"), ("f3
 REGISTRY = {
     ("cast", "generic"): (Cast, _CAST_PAIRS),
     ("beamformer", "ata"): (BeamformerATA, {("cf32", "cf32")}),
+    ("beamformer", "meerkat"): (BeamformerMeerKAT, {("cf32", "cf32")}),
     ("channelizer", "generic"): (Channelizer, {("cf32", "cf32")}),
     ("polarizer", "generic"): (Polarizer, {("cf32", "cf32"), ("cf16", "cf16")}),
     ("detector", "generic"): (Detector, {("cf32", "f32")}),

@@ -98,6 +98,20 @@ BLADE_API int blade_beamform_f32(const void* in, const void* phasors, void* out,
                        int incoherent, int incoherent_sqrt, blade_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * MeerKAT FP32 beamformer:
+ *   out[b,f,t,p] = sum_a in[a,f,t,p] * phasors[b*A + a]   (no conjugate)
+ * one weight per (beam, antenna), shared by every channel and polarisation: the
+ * first B*A values of the phasor buffer, as the reference kernel reads them.
+ * in: CF32 [A,F,T,P]; out: CF32 [B+inc,F,T,P]; incoherent != 0 sizes beam B,
+ * which the reference allocates but never writes; here it is zero.
+ * Replaces Modules::Beamformer::MeerKAT<CF32,CF32> (src/modules/beamformer/
+ * meerkat.cc:8-39) and its kernel src/modules/beamformer/beamformer.cu:81-117.
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_beamform_meerkat_f32(const void* in, const void* phasors, void* out,
+                               uint64_t B, uint64_t A, uint64_t F, uint64_t T,
+                               uint64_t P, int incoherent, blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Channelizer: [A,F,T,P] CF32 -> [A,F*rate,T/rate,P] CF32,
  *   out[a, f*rate + k, s, p] = fftshift(FFT_rate(in[a, f, s*rate:(s+1)*rate, p]))[k]
  * unnormalised, hand-written FP32 Stockham FFT.  rate = 1 copies (or is a no-op

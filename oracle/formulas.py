@@ -113,6 +113,26 @@ def beamform(x: np.ndarray, phasors: np.ndarray, incoherent: bool = False,
     return np.concatenate([y, inc[None].astype(np.complex128)], axis=0)
 
 
+def beamform_meerkat(x: np.ndarray, phasors: np.ndarray, beams: int, incoherent: bool = False) -> np.ndarray:
+    """MeerKAT beamformer: y[b, f, t, p] = sum_a x[a, f, t, p] * w[b*A + a].
+
+    Follows ``src/modules/beamformer/beamformer.cu:81-117``: the kernel reads the
+    phasor buffer as a flat [B, A] array (index ``iy`` runs over beams then
+    antennas), one weight per (beam, antenna) for every channel and polarisation,
+    i.e. the first B*A values of the [B, A, F, 1, P] phasor tensor it is given.
+    The output has B(+1) beams (``include/blade/modules/beamformer/meerkat.hh:17-24``);
+    the kernel never writes the incoherent beam, which is returned as zeros here.
+    """
+    x = np.asarray(x, dtype=np.complex128)
+    A, F, T, P = x.shape
+    B = int(beams)
+    w = np.asarray(phasors, dtype=np.complex128).reshape(-1)[: B * A].reshape(B, A)
+    y = np.einsum("ba,aftp->bftp", w, x)
+    if incoherent:
+        y = np.concatenate([y, np.zeros((1, F, T, P), dtype=np.complex128)], axis=0)
+    return y
+
+
 # --------------------------------------------------------------------------- #
 # Channelizer
 # --------------------------------------------------------------------------- #

@@ -1,6 +1,6 @@
-// C++ bundles: Bundles::ATA::ModeB and Bundles::Generic::ModeH connected to a
-// Pipeline like the reference's C++ examples (examples/pipeline-cpp), one block
-// each.  Writes every case's inputs and outputs as raw little-endian arrays into
+// C++ bundles: Bundles::ATA::ModeB and Bundles::Generic::ModeH (and the
+// Beamformer::MeerKAT module) connected to a Pipeline like the reference's C++
+// examples (examples/pipeline-cpp), one block each.  Writes every case's inputs and outputs as raw little-endian arrays into
 // the directory given as argv[1] (<case>_in.bin, <case>_ph.bin, <case>_out.bin)
 // and prints one JSON line per case; tests/test_cpp.py compares the outputs with
 // the FP64 oracle.
@@ -110,6 +110,24 @@ static bool mode_h(const std::string& dir, const std::string& name, U64 A, U64 F
     return run<Bundle>(p, dir, name, b->getOutputBuffer(), b->isFused());
 }
 
+static bool meerkat(const std::string& dir, uint32_t seed) {
+    const U64 A = 6, F = 3, T = 128, B = 4;
+    ArrayTensor<Device::CUDA, CF32> in(ArrayShape({A, F, T, 2}));
+    PhasorTensor<Device::CUDA, CF32> ph(PhasorShape({B, A, F, 1, 2}));
+    fill(in, seed);
+    phasors(ph, seed + 1);
+    Pipeline p;
+    std::shared_ptr<Modules::Beamformer::MeerKAT<CF32, CF32>> bf;
+    try {
+        p.connect(bf, {.enableIncoherentBeam = true}, {in, ph});
+    } catch (const Error& e) {
+        std::fprintf(stderr, "meerkat: construction failed: %s\n", e.what());
+        return false;
+    }
+    if (!dump(dir + "/meerkat_in.bin", in) || !dump(dir + "/meerkat_ph.bin", ph)) return false;
+    return run<void>(p, dir, "meerkat", bf->getOutputBuffer(), false);
+}
+
 int main(int argc, char** argv) {
     if (argc < 2) {
         std::fprintf(stderr, "usage: test_bundles <out-dir>\n");
@@ -122,5 +140,6 @@ int main(int argc, char** argv) {
     ok &= mode_b<CI8, CF32>(dir, "modeb_ci8_beams", 8, 4, 256, 2, 2, false, true, false, 1, 1, 13);
     ok &= mode_h<CI8, F32>(dir, "modeh_ci8_65536", 1, 2, 65536, true, 1, 4, 14);
     ok &= mode_h<CF32, F32>(dir, "modeh_cf32_1024", 2, 3, 1024, false, 1, 1, 15);
+    ok &= meerkat(dir, 16);
     return ok ? 0 : 1;
 }

@@ -62,7 +62,7 @@ def test_cpp_bundles_match_oracle(cuda, tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
     fused = {d["case"]: d["fused"] for d in (json.loads(line) for line in r.stdout.strip().splitlines())}
     assert fused == {"modeb_ci8_r4": False, "modeb_cf32_r1": True, "modeb_ci8_beams": False,
-                     "modeh_ci8_65536": True, "modeh_cf32_1024": False}
+                     "modeh_ci8_65536": True, "modeh_cf32_1024": False, "meerkat": False}
 
     def rel(a, b):
         return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
@@ -94,3 +94,8 @@ def test_cpp_bundles_match_oracle(cuda, tmp_path):
     got = _read(tmp_path / "modeh_cf32_1024_out.bin", np.float32, (2, 3 * 1024, 1, 1))
     ref = O.detect(O.channelize(x, 1024), 1, 1)
     assert rel(got, ref) < 1e-5
+    # Beamformer::MeerKAT: one weight per (beam, antenna), incoherent beam zero
+    x, w = cf32("meerkat", 6, 3, 128), _read(tmp_path / "meerkat_ph.bin", np.complex64, (4, 6, 3, 1, 2))
+    got = _read(tmp_path / "meerkat_out.bin", np.complex64, (5, 3, 128, 2))
+    ref = O.beamform_meerkat(x, w, 4, incoherent=True)
+    assert rel(got[:4], ref[:4]) < 1e-5 and np.all(got[4] == 0)

@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 import torch
 
+import blade_b200 as bl
 from oracle import formulas as O
 from blade_b200 import _lib, synthetic as S
 from tests.gpu_util import c64, call, crand, dev, host, ptr, rel_l2, stream
@@ -80,6 +81,38 @@ def test_beamformer_f32(cuda, A, F, T, P, B, inc, sq):
     if inc:
         assert rel_l2(y[B], ref[B]) < TOL
         assert np.all(y[B].imag == 0)
+
+
+@pytest.mark.parametrize("A,F,T,P,B,inc", [(16, 4, 512, 2, 8, True), (64, 3, 1024, 2, 64, False),
+                                           (3, 5, 77, 1, 5, True), (7, 2, 64, 2, 2, False)])
+def test_beamformer_meerkat(cuda, A, F, T, P, B, inc):
+    # src/modules/beamformer/beamformer.cu:81-117: weight w[b*A + a] of a [B, A, F, 1, P] tensor
+    rng = np.random.default_rng(A * 7 + B)
+    x = crand(rng, (A, F, T, P))
+    w = crand(rng, (B, A, F, 1, P))
+    xd, wd = c64(x), c64(w)
+    yd = torch.full((B + int(inc), F, T, P), 7.0, dtype=torch.complex64, device="cuda")
+    call("blade_beamform_meerkat_f32", ptr(xd), ptr(wd), ptr(yd), B, A, F, T, P, int(inc), stream())
+    y = host(yd)
+    ref = O.beamform_meerkat(x, w, B, inc)
+    assert rel_l2(y[:B], ref[:B]) < TOL
+    if inc:
+        assert np.all(y[B] == 0)
+
+
+def test_beamformer_meerkat_module(cuda):
+    A, F, T, P, B = 8, 4, 256, 2, 3
+    rng = np.random.default_rng(5)
+    x, w = crand(rng, (A, F, T, P)), crand(rng, (B, A, F, 1, P))
+    buf = bl.array_tensor((A, F, T, P), dtype=bl.cf32, device=bl.cuda)
+    ph = bl.phasor_tensor((B, A, F, 1, P), dtype=bl.cf32, device=bl.cuda)
+    buf.as_torch().copy_(c64(x))
+    ph.as_torch().copy_(c64(w))
+    mod = bl.module(bl.beamformer, {"enable_incoherent_beam": False}, (buf, ph), telescope=bl.meerkat)
+    assert isinstance(mod, bl.BeamformerMeerKAT)
+    mod.process()
+    torch.cuda.synchronize()
+    assert rel_l2(mod.get_output().as_torch().cpu().numpy(), O.beamform_meerkat(x, w, B)) < TOL
 
 
 # ------------------------------------------------------------------------ channelizer

@@ -186,3 +186,21 @@ def test_mode_b_incoherent_beam_is_square_rooted_before_the_detector():
     np.testing.assert_allclose(out[2, :, :, 0], ref, rtol=1e-12)
     stepwise = O.detect(O.beamform(y, w), 2, 1)
     np.testing.assert_allclose(out[:2], stepwise, rtol=1e-12)
+
+
+def test_beamform_meerkat_reads_flat_beam_antenna_weights():
+    # src/modules/beamformer/beamformer.cu:103-114: iy runs 0, 1, ... over (beam, antenna)
+    rng = np.random.default_rng(15)
+    A, F, T, P, B = 3, 2, 4, 2, 2
+    x = crand(rng, (A, F, T, P))
+    w = crand(rng, (B, A, F, 1, P))
+    flat = w.reshape(-1)
+    out = O.beamform_meerkat(x, w, B, incoherent=True)
+    assert out.shape == (B + 1, F, T, P)
+    for b in range(B):
+        for f in range(F):
+            for t in range(T):
+                for p in range(P):
+                    ref = sum(x[a, f, t, p] * flat[b * A + a] for a in range(A))
+                    np.testing.assert_allclose(out[b, f, t, p], ref, rtol=1e-12)
+    assert np.all(out[B] == 0)
