@@ -27,7 +27,7 @@ def test_module_dispatch_errors():
     with pytest.raises(ValueError):
         bl.module("beamformer", {}, None)
     with pytest.raises(AttributeError, match="telescopes"):
-        bl.module(bl.beamformer, {}, None, telescope=bl.meerkat)
+        bl.module(bl.beamformer, {}, None, telescope=bl.vla)
     with pytest.raises(AttributeError, match="generic telescopes"):
         bl.module(bl.detector, {}, None, telescope=bl.ata)
     with pytest.raises(AttributeError, match="input types"):
