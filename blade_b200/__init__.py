@@ -26,6 +26,7 @@ from .memory import copy as _mem_copy
 from .modules import (BeamformDetect, BeamformerATA, BeamformerMeerKAT, Cast, Channelizer, Detector, Duplicate,
                       Gather, ModeB, ModeH, Module, Permutation, Phasor, Polarizer)
 from .runtime import Pipeline, Runner, module, runner
+from .guppi import GuppiReader, GuppiWriter
 
 __version__ = "1.0.0"
 
