@@ -18,8 +18,11 @@ through the public Runner API with host buffers.  Three further legs cover the
 other measured workloads: the high-resolution spectrometer (A = 1, F = 64,
 T = 2^20, Cast -> Channelizer(65536) -> Polarizer -> Detector I = 8), the small
 block's launch latency eager against one CUDA graph (A = 20, F = 96, T = 256,
-B = 8), and the forward + adjoint step of the Stokes loss (A = 28, B = 1,
-F = 192, T = 2048, CF32); --skip-extra leaves them out.
+B = 8; also as one fused FP32 launch and as the tensor-core pair), the forward +
+adjoint step of the Stokes loss (A = 28, B = 1, F = 192, T = 2048, CF32) and the
+ATA ModeB bundle in the reference's order on the production block
+(pre-beamformer channelizer, per-fine-channel phasors, incoherent beam);
+--skip-extra leaves them out.
 
 Multi-GPU (torchrun): weak scaling, every rank owns its own 192-channel band
 (frequency sharding, no data-path collective); time = max over ranks.
@@ -397,9 +400,10 @@ def spectrometer(steps, warmup):
 
 def small_block_latency(calls):
     """Small ATA block (A=20 F=96 T=256 P=2 B=8, I=4): Cast -> Beamformer(FP32) -> Detector,
-    three launches per call, eager against one CUDA graph replay.  Reports the host
-    wall time of one call waited to completion (latency) and the device time per call
-    when calls are issued back to back (throughput)."""
+    three launches per call, eager against one CUDA graph replay; then the same chain
+    as one fused FP32 launch and as the tensor-core pair (phasor split + fused kernel).
+    Reports the host wall time of one call waited to completion (latency) and the
+    device time per call when calls are issued back to back (throughput)."""
     from blade_b200 import _lib
 
     _lib.load()
@@ -413,44 +417,99 @@ def small_block_latency(calls):
     out = torch.empty((B, F, T // I, 1), dtype=torch.float32, device="cuda")
     side = torch.cuda.Stream()
 
+    lib = _lib.load()
+    plan = torch.empty(int(lib.blade_beamform_tc_plan_size(B, A, F, P)), dtype=torch.uint8, device="cuda")
+    out2 = torch.empty_like(out)
+
     def call(sh):
         _lib.call("blade_cast", _lib.CI8, _lib.CF32, x.data_ptr(), xf.data_ptr(), A * F * T * P, sh)
         _lib.call("blade_beamform_f32", xf.data_ptr(), ph.data_ptr(), y.data_ptr(), B, A, F, T, P, 0, 0, sh)
         _lib.call("blade_detect", y.data_ptr(), out.data_ptr(), B, F, T, P, I, 1, sh)
 
+    def call_f32(sh):  # the same chain as one fused FP32 launch (CI8 in, Stokes-I out)
+        _lib.call("blade_beamform_detect_f32", _lib.CI8, x.data_ptr(), ph.data_ptr(), out2.data_ptr(), B, A, F, T, P,
+                  1, I, sh)
+
+    def call_tc(sh):  # phasor split + the tensor-core chain: two launches
+        _lib.call("blade_beamform_tc_prepare", ph.data_ptr(), plan.data_ptr(), B, A, F, P, sh)
+        _lib.call("blade_beamform_detect_tc", x.data_ptr(), plan.data_ptr(), out2.data_ptr(), B, A, F, T, P, 1, I, sh)
+
+    res = {"workload": "A=20 F=96 T=256 P=2 B=8 I=4, Cast->Beamformer(FP32)->Detector, 3 launches"}
     with torch.cuda.stream(side):
         sh = side.cuda_stream
-        for _ in range(10):
-            call(sh)
-        torch.cuda.synchronize()
-        graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(graph, stream=side):
-            call(torch.cuda.current_stream().cuda_stream)
-        torch.cuda.synchronize()
+        for label, fn in (("", call), ("fused_f32_", call_f32), ("fused_tc_", call_tc)):
+            for _ in range(10):
+                fn(sh)
+            torch.cuda.synchronize()
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=side):
+                fn(torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            eager_lat, eager_dev = _measure_calls(lambda: fn(sh), side, calls)
+            graph_lat, graph_dev = _measure_calls(graph.replay, side, calls)
+            del graph
+            res.update({f"{label}eager_us_per_call": round(eager_lat, 2), f"{label}graph_us_per_call": round(graph_lat, 2),
+                        f"{label}eager_device_us_per_call": round(eager_dev, 2),
+                        f"{label}graph_device_us_per_call": round(graph_dev, 2)})
+            if not label:
+                res["graph_tmacs"] = round(4 * B * A * F * T * P / (graph_dev * 1e-6) / 1e12, 4)
+    res["fused_rel_l2_vs_chain"] = float((out2 - out).norm() / out.norm())
+    return res
 
-        def measure(fn):
-            lat = []
-            for _ in range(calls):
-                t = time.perf_counter()
-                fn()
-                side.synchronize()
-                lat.append(time.perf_counter() - t)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(side)
-            for _ in range(calls):
-                fn()
-            e1.record(side)
-            side.synchronize()
-            return float(np.median(lat)) * 1e6, e0.elapsed_time(e1) * 1e3 / calls
 
-        eager_lat, eager_dev = measure(lambda: call(sh))
-        graph_lat, graph_dev = measure(graph.replay)
-    del graph
-    mac = 4 * B * A * F * T * P
-    return {"workload": "A=20 F=96 T=256 P=2 B=8 I=4, Cast->Beamformer(FP32)->Detector, 3 launches",
-            "eager_us_per_call": round(eager_lat, 2), "graph_us_per_call": round(graph_lat, 2),
-            "eager_device_us_per_call": round(eager_dev, 2), "graph_device_us_per_call": round(graph_dev, 2),
-            "graph_tmacs": round(mac / (graph_dev * 1e-6) / 1e12, 4)}
+def _measure_calls(fn, side, calls):
+    """Median host wall time of one call waited to completion, and device time per
+    call back to back (CUDA events on the launching stream), in microseconds."""
+    lat = []
+    for _ in range(calls):
+        t = time.perf_counter()
+        fn()
+        side.synchronize()
+        lat.append(time.perf_counter() - t)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(side)
+    for _ in range(calls):
+        fn()
+    e1.record(side)
+    side.synchronize()
+    return float(np.median(lat)) * 1e6, e0.elapsed_time(e1) * 1e3 / calls
+
+
+def modeb_step(steps, warmup):
+    """ATA ModeB in the reference's own order (include/blade/bundles/ata/mode_b.hh:99-199)
+    on the production block: Cast -> Channelizer(rate 4) -> Beamformer with per-fine-
+    channel phasors and the incoherent beam -> Detector (Stokes-I, I=4), CI8 in, through
+    bl.module(bl.modeb).  Four module launches per step (no fused kernel covers
+    per-fine-channel phasors)."""
+    import blade_b200 as bl
+
+    w = dict(WORK)
+    A, F, T, P, B, R, I = (w[k] for k in ("A", "F", "T", "P", "B", "R", "I"))
+    g = torch.Generator(device="cuda").manual_seed(1006)
+    buf = bl.array_tensor((A, F, T, P), dtype=bl.ci8, device=bl.cuda)
+    buf.as_torch().copy_((torch.randn((A, F, T, P, 2), generator=g, device="cuda") * 8).round_().clamp_(-127, 127))
+    ph = bl.phasor_tensor((B, A, F * R, 1, P), dtype=bl.cf32, device=bl.cuda)
+    ph.as_torch().copy_(torch.polar(torch.ones((B, A, F * R, 1, P), device="cuda"),
+                                    torch.rand((B, A, F * R, 1, P), generator=g, device="cuda") * 6.283185307))
+    cfg = {"input_shape": (A, F, T, P), "output_shape": (B + 1, F * R, T // (R * I), 1),
+           "pre_beamformer_channelizer_rate": R, "beamformer_incoherent_beam": True, "detector_enable": True,
+           "detector_integration_size": I, "detector_number_of_output_polarizations": 1}
+    mod = bl.module(bl.modeb, cfg, {"buffer": buf, "phasors": ph}, it=bl.ci8, ot=bl.f32, telescope=bl.ata)
+    s = torch.cuda.current_stream()
+    for _ in range(warmup):
+        mod.process(0, s)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(steps):
+        mod.process(0, s)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    del mod, buf, ph
+    return {"workload": "A=28 F=192 T=8192 P=2 B=16 (+ incoherent), Cast->Channelizer(4)->Beamformer(fine phasors)"
+                        "->Detector(Stokes-I, I=4)",
+            "ms_per_step": round(ms, 4), "tmacs": round(tmac(w) / (ms * 1e-3) / 1e12, 3)}
 
 
 def adjoint_step(steps, warmup):
@@ -548,6 +607,7 @@ def run_ours(args):
             extra["spectrometer"] = spectrometer(max(3, args.steps // 6), args.warmup)
             extra["small_block_latency"] = small_block_latency(200)
             extra["adjoint"] = adjoint_step(max(5, args.steps // 2), args.warmup)
+            extra["modeb"] = modeb_step(max(3, args.steps // 6), args.warmup)
         torch.cuda.synchronize()
     clocks = clk.summary()
     if rank != 0:
