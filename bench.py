@@ -605,7 +605,7 @@ def run_ours(args):
         extra = {}
         if not args.skip_extra and world == 1:
             extra["spectrometer"] = spectrometer(max(3, args.steps // 6), args.warmup)
-            extra["small_block_latency"] = small_block_latency(200)
+            extra["small_block_latency"] = small_block_latency(100)
             extra["adjoint"] = adjoint_step(max(5, args.steps // 2), args.warmup)
             extra["modeb"] = modeb_step(max(3, args.steps // 6), args.warmup)
         torch.cuda.synchronize()

@@ -15,6 +15,8 @@
 // in registers.  The slices are added in a fixed order at the end, the chunks by a
 // second kernel and the loss by a third, so results are deterministic.  HBM traffic
 // is one read of the voltages.  Other shapes take the one-CTA-per-(f, p) kernel.
+#include <mutex>
+
 #include "common.cuh"
 #include "tc_ptx.cuh"
 
@@ -298,6 +300,40 @@ __global__ void __launch_bounds__(256) loss_sum_kernel(const double* __restrict_
     if (threadIdx.x == 0) *loss = -sh[0];
 }
 
+// Stream-ordered scratch comes from a pool owned by the library, one per device,
+// that keeps its memory between calls (release threshold = max): steady-state
+// calls reuse it and never reach the driver's allocator, which the default pool
+// (threshold 0) does again after every synchronisation.
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaMallocAsync(p, bytes, s);
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!pools[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            e = cudaMemPoolCreate(&pool, &props);
+            if (e != cudaSuccess) return e;
+            uint64_t keep = ~0ull;
+            e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            if (e != cudaSuccess) {
+                cudaMemPoolDestroy(pool);
+                return e;
+            }
+            pools[dev] = pool;
+        }
+        pool = pools[dev];
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, s);
+}
+
 }  // namespace
 }  // namespace bb
 
@@ -327,8 +363,8 @@ extern "C" int blade_beamform_detect_adjoint(const void* in, const void* phasors
         nch = (ntiles + tpc - 1) / tpc;
         float4* gpart = nullptr;
         double* lpart = nullptr;
-        cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&gpart), F * nch * Q * sizeof(float4), s);
-        if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&lpart), F * nch * sizeof(double), s);
+        cudaError_t e = scratch_alloc(reinterpret_cast<void**>(&gpart), F * nch * Q * sizeof(float4), s);
+        if (e == cudaSuccess) e = scratch_alloc(reinterpret_cast<void**>(&lpart), F * nch * sizeof(double), s);
         if (e != cudaSuccess) {
             if (gpart) cudaFreeAsync(gpart, s);
             return check_cuda(e, "blade_beamform_detect_adjoint (scratch)");
@@ -365,7 +401,7 @@ extern "C" int blade_beamform_detect_adjoint(const void* in, const void* phasors
                          (unsigned long long)B, (unsigned long long)A);
     double* lpart = nullptr;
     if (loss) {
-        cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&lpart), F * P * sizeof(double), s);
+        cudaError_t e = scratch_alloc(reinterpret_cast<void**>(&lpart), F * P * sizeof(double), s);
         if (e != cudaSuccess) return check_cuda(e, "blade_beamform_detect_adjoint (scratch)");
     }
     int rc = ensure_smem(reinterpret_cast<const void*>(adjoint_kernel), smem);
