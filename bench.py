@@ -21,7 +21,8 @@ block's launch latency eager against one CUDA graph (A = 20, F = 96, T = 256,
 B = 8; also as one fused FP32 launch and as the tensor-core pair), the forward +
 adjoint step of the Stokes loss (A = 28, B = 1, F = 192, T = 2048, CF32) and the
 ATA ModeB bundle in the reference's order on the production block
-(pre-beamformer channelizer, per-fine-channel phasors, incoherent beam);
+(pre-beamformer channelizer, per-fine-channel phasors; tensor-core path, and the
+module chain with the incoherent beam);
 --skip-extra leaves them out.
 
 Multi-GPU (torchrun): weak scaling, every rank owns its own 192-channel band
@@ -478,9 +479,11 @@ def _measure_calls(fn, side, calls):
 def modeb_step(steps, warmup):
     """ATA ModeB in the reference's own order (include/blade/bundles/ata/mode_b.hh:99-199)
     on the production block: Cast -> Channelizer(rate 4) -> Beamformer with per-fine-
-    channel phasors and the incoherent beam -> Detector (Stokes-I, I=4), CI8 in, through
-    bl.module(bl.modeb).  Four module launches per step (no fused kernel covers
-    per-fine-channel phasors)."""
+    channel phasors -> Detector (Stokes-I, I=4), CI8 in, through bl.module(bl.modeb).
+    Without the incoherent beam (as the reference's ModeB test runs it) the bundle takes
+    the tensor-core path (pre-beamformer stages into exact FP16, then the tensor-core
+    chain on the 768 fine channels: three launches); with it, the module chain (five
+    launches)."""
     import blade_b200 as bl
 
     w = dict(WORK)
@@ -491,25 +494,33 @@ def modeb_step(steps, warmup):
     ph = bl.phasor_tensor((B, A, F * R, 1, P), dtype=bl.cf32, device=bl.cuda)
     ph.as_torch().copy_(torch.polar(torch.ones((B, A, F * R, 1, P), device="cuda"),
                                     torch.rand((B, A, F * R, 1, P), generator=g, device="cuda") * 6.283185307))
-    cfg = {"input_shape": (A, F, T, P), "output_shape": (B + 1, F * R, T // (R * I), 1),
-           "pre_beamformer_channelizer_rate": R, "beamformer_incoherent_beam": True, "detector_enable": True,
-           "detector_integration_size": I, "detector_number_of_output_polarizations": 1}
-    mod = bl.module(bl.modeb, cfg, {"buffer": buf, "phasors": ph}, it=bl.ci8, ot=bl.f32, telescope=bl.ata)
     s = torch.cuda.current_stream()
-    for _ in range(warmup):
-        mod.process(0, s)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(s)
-    for _ in range(steps):
-        mod.process(0, s)
-    e1.record(s)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    del mod, buf, ph
-    return {"workload": "A=28 F=192 T=8192 P=2 B=16 (+ incoherent), Cast->Channelizer(4)->Beamformer(fine phasors)"
-                        "->Detector(Stokes-I, I=4)",
-            "ms_per_step": round(ms, 4), "tmacs": round(tmac(w) / (ms * 1e-3) / 1e12, 3)}
+    res = {"workload": "A=28 F=192 T=8192 P=2 B=16, Cast->Channelizer(4)->Beamformer(fine phasors)"
+                       "->Detector(Stokes-I, I=4)"}
+    outs = {}
+    for label, inc in (("", False), ("incoherent_", True)):
+        cfg = {"input_shape": (A, F, T, P), "output_shape": (B + int(inc), F * R, T // (R * I), 1),
+               "pre_beamformer_channelizer_rate": R, "beamformer_incoherent_beam": inc, "detector_enable": True,
+               "detector_integration_size": I, "detector_number_of_output_polarizations": 1}
+        mod = bl.module(bl.modeb, cfg, {"buffer": buf, "phasors": ph}, it=bl.ci8, ot=bl.f32, telescope=bl.ata)
+        for _ in range(warmup):
+            mod.process(0, s)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(steps):
+            mod.process(0, s)
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        res[f"{label}path"] = "tensor cores" if mod.tensor_cores else "module chain"
+        res[f"{label}ms_per_step"] = round(ms, 4)
+        res[f"{label}tmacs"] = round(tmac(w) / (ms * 1e-3) / 1e12, 3)
+        outs[label] = mod.get_output().as_torch()[:B].clone()
+        del mod
+    res["tc_vs_chain_rel_l2"] = float((outs[""] - outs["incoherent_"]).norm() / outs["incoherent_"].norm())
+    del buf, ph, outs
+    return res
 
 
 def adjoint_step(steps, warmup):

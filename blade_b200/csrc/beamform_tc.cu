@@ -329,6 +329,36 @@ __device__ __forceinline__ void r4_pair_task(const uint8_t* raw, uint32_t rrow, 
     }
 }
 
+// Rate 1 from CF16 voltages (the ModeB path: channelized and polarized on the
+// way in, exact in FP16): raw rows of 128 samples x 8 bytes [p0 (re, im) | p1 (re,
+// im)] per antenna.  A task is one sample of 8 antennas -> the (re, im) chunks of
+// polarisation p; consecutive lanes take consecutive samples (rows).
+__device__ __forceinline__ void build_operand_h16(const uint8_t* raw, uint32_t rrow, uint8_t* op, uint32_t A,
+                                                  uint32_t KA, int p, uint32_t ct) {
+    constexpr uint32_t kStride = kConvWarps * 32;
+    const uint32_t ntasks = kM * (KA / 8);
+    for (uint32_t t = ct; t < ntasks; t += kStride) {
+        const uint32_t s = t % kM, g = t / kM;
+        uint32_t h[8];  // half2 (re, im) of polarisation p, antennas g*8 .. g*8+7
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const uint32_t a = g * 8 + i;
+            h[i] = a < A ? *reinterpret_cast<const uint32_t*>(raw + a * rrow + s * 8 + p * 4) : 0u;
+        }
+        uint4 vr, vi;
+        vr.x = __byte_perm(h[0], h[1], 0x5410);
+        vr.y = __byte_perm(h[2], h[3], 0x5410);
+        vr.z = __byte_perm(h[4], h[5], 0x5410);
+        vr.w = __byte_perm(h[6], h[7], 0x5410);
+        vi.x = __byte_perm(h[0], h[1], 0x7632);
+        vi.y = __byte_perm(h[2], h[3], 0x7632);
+        vi.z = __byte_perm(h[4], h[5], 0x7632);
+        vi.w = __byte_perm(h[6], h[7], 0x7632);
+        *reinterpret_cast<uint4*>(op + op_off(s, g * 8)) = vr;
+        *reinterpret_cast<uint4*>(op + op_off(s, KA + g * 8)) = vi;
+    }
+}
+
 // Both polarisations of one tile for R = 1 and 2: two single-polarisation passes.
 template <int R>
 __device__ __forceinline__ void build_operand_pair(const uint8_t* raw, uint32_t rrow, uint8_t* op0, uint8_t* op1, uint32_t A,
@@ -402,7 +432,8 @@ __device__ __forceinline__ void issue_ka32(uint32_t d, uint64_t ad, uint64_t wd,
             mma_f16(d, a_step(ad, j), wd + (uint64_t)(h * 2 * nb16 + j * 2), idesc, (h | j) ? 1u : 0u);
 }
 
-template <int R, int LOGI>
+// ES = bytes per dual-polarisation input sample: 4 (CI8) or 8 (CF16, rate 1 only).
+template <int R, int LOGI, int ES = 4>
 __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, const __grid_constant__ CUtensorMap tmap) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // Swizzled operands need 1024-byte aligned atoms: align the working base.
@@ -580,7 +611,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
             // two TMA boxes of up to 256 samples x 1 channel x A antennas (rows of
             // raw_row bytes per antenna: 512-byte rows per tile leave DRAM bandwidth
             // unused, 1-2 KB rows do not).
-            const uint32_t RT = g.raw_tiles, box = g.raw_row / 4, nbox = RT * kM / box;
+            const uint32_t RT = g.raw_tiles, box = g.raw_row / ES, nbox = RT * kM / box;
             uint32_t f = (uint32_t)(L0 / tpc), tt = (uint32_t)(L0 % tpc);  // stepped below
             for (uint64_t L = L0; L < L1; L += RT) {
                 int ok = 1;
@@ -602,7 +633,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
                 if (lane == 0) {
                     ok = mbar_wait(&r_empty[rs], rph ^ 1, abort, kWaitBudget);
                     if (ok) {
-                        mbar_arrive_expect_tx(&r_full[rs], g.A * 512u * RT);
+                        mbar_arrive_expect_tx(&r_full[rs], g.A * (uint32_t)(kM * ES) * RT);
                         uint8_t* dst = r_smem + (size_t)rs * g.raw_bytes;
                         for (uint32_t b = 0; b < nbox; b++)
                             tma_load_3d(dst + (size_t)b * g.A * g.raw_row, &tmap, (int)(tt * kM + b * box), (int)f, 0,
@@ -763,8 +794,8 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
                 if (!mbar_wait(&r_full[rs], rph, abort, kWaitBudget)) { record_abort(abort, 11); break; }
             }
             // this tile inside the stage: box (sub * 128 / box), column (sub * 128 % box)
-            const uint32_t sb = sub * kM, box = g.raw_row / 4;
-            const uint8_t* raw = r_smem + (size_t)rs * g.raw_bytes + (sb / box) * g.A * g.raw_row + (sb % box) * 4u;
+            const uint32_t sb = sub * kM, box = g.raw_row / ES;
+            const uint8_t* raw = r_smem + (size_t)rs * g.raw_bytes + (sb / box) * g.A * g.raw_row + (sb % box) * ES;
             if (pair) {
                 // Both polarisations in one pass into stages as, as + 1 (AS is even).
                 if (!mbar_wait(&a_empty[as + 1], aph ^ 1, abort, kWaitBudget)) {
@@ -777,6 +808,9 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
 #pragma unroll
                     for (uint32_t i = 0; i < kMaxT4; i++)
                         if (i < nt4) r4_pair_task(raw, g.raw_row, op0, op1, t4[i]);
+                } else if constexpr (ES == 8) {
+                    build_operand_h16(raw, g.raw_row, op0, g.A, KA, 0, ct);
+                    build_operand_h16(raw, g.raw_row, op1, g.A, KA, 1, ct);
                 } else {
                     build_operand_pair<R>(raw, g.raw_row, op0, op1, g.A, KA, ct);
                 }
@@ -788,7 +822,8 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
             } else {
                 for (int p = 0; p < 2; p++) {
                     if (!mbar_wait(&a_empty[as], aph ^ 1, abort, kWaitBudget)) { record_abort(abort, 8); ok = false; break; }
-                    build_operand<R>(raw, g.raw_row, a_smem + (size_t)as * op_bytes, g.A, KA, p, ct);
+                    if constexpr (ES == 8) build_operand_h16(raw, g.raw_row, a_smem + (size_t)as * op_bytes, g.A, KA, p, ct);
+                    else build_operand<R>(raw, g.raw_row, a_smem + (size_t)as * op_bytes, g.A, KA, p, ct);
                     fence_proxy_async_smem();
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&a_full[as]);
@@ -920,7 +955,7 @@ struct TcShape {
 };
 
 // T = 0 sizes only the phasor image (the ring layout needs the tiles per channel).
-bool tc_shape(uint64_t B, uint64_t A, TcShape& s, uint64_t T = 0) {
+bool tc_shape(uint64_t B, uint64_t A, TcShape& s, uint64_t T = 0, uint32_t es = 4) {
     if (A == 0 || A > kMaxKA || B == 0) return false;
     const uint64_t bc = B < (uint64_t)kMaxNB ? B : (uint64_t)kMaxNB;
     s.NB = (uint32_t)((bc + 15) / 16 * 16);
@@ -930,7 +965,7 @@ bool tc_shape(uint64_t B, uint64_t A, TcShape& s, uint64_t T = 0) {
     // doubled accumulators still fit twice in tensor memory.
     s.stacked = s.NB <= 32 ? 1u : 0u;
     s.img_bytes = s.stacked ? (2 * s.KA / 64) * 1024u * s.NB : (s.KA == 64 ? 1536u : 1024u) * s.NB;
-    s.raw_bytes = (uint32_t)A * 512u;
+    s.raw_bytes = (uint32_t)A * kM * es;
     const size_t op = (2ull * s.KA / 64) * 16384;   // one polarisation's operand
     // barriers (2 x 8 operand + 2 x 8 raw + 2 x 4 accumulator + 3, 8 bytes each),
     // TMEM slot and abort flag, alignment slack
@@ -941,7 +976,22 @@ bool tc_shape(uint64_t B, uint64_t A, TcShape& s, uint64_t T = 0) {
     // operand build runs up to four tiles ahead of the MMAs), else two pairs and
     // four or three raw stages.
     const uint64_t tpc = T / kM;
-    if (T && tpc % 2 == 0) {
+    if (T && es == 8) {
+        // CF16 input: single-tile raw stages of 1 KB rows; four operand pairs and two
+        // raw stages (two issuers), else two pairs and four or three raw stages.
+        const uint32_t cand[][2] = {{8, 2}, {4, 4}, {4, 3}};
+        for (const auto& c : cand) {
+            if (fixed + c[0] * op + c[1] * (size_t)s.raw_bytes <= limit) {
+                s.raw_tiles = 1;
+                s.raw_row = kM * es;
+                s.a_stages = c[0];
+                s.r_stages = c[1];
+                s.smem = fixed + c[0] * op + c[1] * (size_t)s.raw_bytes;
+                return true;
+            }
+        }
+    }
+    if (T && es == 4 && tpc % 2 == 0) {
         const size_t raw2 = (size_t)A * 1024u;
         const uint32_t cand[][2] = {{8, 2}, {4, 4}, {4, 3}};
         for (const auto& c : cand) {
@@ -957,7 +1007,7 @@ bool tc_shape(uint64_t B, uint64_t A, TcShape& s, uint64_t T = 0) {
         }
     }
     s.raw_tiles = 1;
-    s.raw_row = 512;
+    s.raw_row = kM * es;
     // Deepest rings that fit: operand stages in pairs (one per polarisation) down to
     // four, raw stages down to three, then both down to the minimum.
     uint32_t as = kMaxStages, rs = 6;
@@ -977,9 +1027,11 @@ bool tc_shape(uint64_t B, uint64_t A, TcShape& s, uint64_t T = 0) {
 
 using TcKernel = void (*)(const TcArgs, const CUtensorMap);
 
-// Tensor map of the CI8 voltages seen as uint32 samples [A][F][T] (one 4-byte
-// word = both polarisations of one sample); box = `box` samples x 1 channel x A.
-int encode_voltage_map(CUtensorMap* tm, const void* in, uint64_t A, uint64_t F, uint64_t T, uint32_t box_t) {
+// Tensor map of the voltages seen as samples [A][F][T] of es bytes (CI8: one
+// 4-byte word, CF16: one 8-byte word = both polarisations of one sample);
+// box = `box` samples x 1 channel x A.
+int encode_voltage_map(CUtensorMap* tm, const void* in, uint64_t A, uint64_t F, uint64_t T, uint32_t box_t,
+                       uint32_t es = 4) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     static std::mutex mu;
     {
@@ -995,10 +1047,10 @@ int encode_voltage_map(CUtensorMap* tm, const void* in, uint64_t A, uint64_t F, 
         }
     }
     const cuuint64_t dims[3] = {T, F, A};
-    const cuuint64_t strides[2] = {T * 4, F * T * 4};
+    const cuuint64_t strides[2] = {T * es, F * T * es};
     const cuuint32_t box[3] = {box_t, 1, (cuuint32_t)A};
     const cuuint32_t estr[3] = {1, 1, 1};
-    const CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, const_cast<void*>(in), dims, strides, box, estr,
+    const CUresult r = encode(tm, es == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, const_cast<void*>(in), dims, strides, box, estr,
                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_error(BLADE_CUDA_ERROR, "blade_beamform_detect_tc: tensor map encode (%d)", (int)r);
@@ -1065,26 +1117,19 @@ extern "C" int blade_beamform_detect_tc_supported(uint64_t B, uint64_t A, uint64
     return 1;
 }
 
-extern "C" int blade_beamform_detect_tc(const void* in, const void* plan, void* out, uint64_t B, uint64_t A,
-                                        uint64_t F, uint64_t T, uint64_t P, uint64_t rate, uint64_t integration,
-                                        blade_stream_t stream) {
-    if (!blade_beamform_detect_tc_supported(B, A, F, T, P, rate, integration))
-        return set_error(BLADE_ERROR,
-                         "blade_beamform_detect_tc: unsupported configuration (B=%llu A=%llu T=%llu P=%llu rate=%llu "
-                         "I=%llu): needs P=2, 1<=A<=64, T%%128==0, rate in {1,2,4}, I a power of two <= 32",
-                         (unsigned long long)B, (unsigned long long)A, (unsigned long long)T, (unsigned long long)P,
-                         (unsigned long long)rate, (unsigned long long)integration);
-    if (!in || !plan || !out) return set_error(BLADE_ERROR, "blade_beamform_detect_tc: null buffer");
-    if (!aligned16(in) || !aligned16(plan) || (reinterpret_cast<uintptr_t>(out) & 3))
-        return set_error(BLADE_ERROR, "blade_beamform_detect_tc: input and plan must be 16-byte aligned");
+namespace bb {
+namespace {
+
+// Launches the chain over the 64-beam chunks once the arguments are checked.
+int tc_run(const char* who, const void* in, const void* plan, void* out, uint64_t B, uint64_t A, uint64_t F,
+           uint64_t T, uint64_t rate, uint64_t integration, uint32_t es, TcKernel fn, blade_stream_t stream) {
     TcShape s;
-    tc_shape(B, A, s, T);
+    tc_shape(B, A, s, T, es);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const TcKernel fn = pick_kernel(rate, integration);
     if (int rc = ensure_smem(reinterpret_cast<const void*>(fn), s.smem)) return rc;
     const uint32_t U = (uint32_t)(T / (rate * integration));
     CUtensorMap tmap;
-    if (int rc = encode_voltage_map(&tmap, in, A, F, T, s.raw_row / 4)) return rc;
+    if (int rc = encode_voltage_map(&tmap, in, A, F, T, s.raw_row / es, es)) return rc;
     for (uint32_t c = 0; c < s.nchunks; c++) {
         TcArgs g;
         g.in = static_cast<const uint8_t*>(in);
@@ -1113,9 +1158,57 @@ extern "C" int blade_beamform_detect_tc(const void* in, const void* plan, void* 
         const uint64_t per = ((g.total_tiles + sms - 1) / sms + s.raw_tiles - 1) / s.raw_tiles * s.raw_tiles;
         const uint64_t grid = (g.total_tiles + per - 1) / per;
         fn<<<(unsigned)grid, kThreads, s.smem, st>>>(g, tmap);
-        if (int rc = check_launch("blade_beamform_detect_tc")) return rc;
+        if (int rc = check_launch(who)) return rc;
     }
     return BLADE_SUCCESS;
+}
+
+TcKernel pick_cf16(uint64_t integration) {
+    uint32_t logi = 0;
+    while ((1ull << logi) < integration) logi++;
+    switch (logi) {
+        case 0: return bf_tc_kernel<1, 0, 8>;
+        case 1: return bf_tc_kernel<1, 1, 8>;
+        case 2: return bf_tc_kernel<1, 2, 8>;
+        case 3: return bf_tc_kernel<1, 3, 8>;
+        case 4: return bf_tc_kernel<1, 4, 8>;
+        default: return bf_tc_kernel<1, 5, 8>;
+    }
+}
+
+}  // namespace
+}  // namespace bb
+
+extern "C" int blade_beamform_detect_tc(const void* in, const void* plan, void* out, uint64_t B, uint64_t A,
+                                        uint64_t F, uint64_t T, uint64_t P, uint64_t rate, uint64_t integration,
+                                        blade_stream_t stream) {
+    if (!blade_beamform_detect_tc_supported(B, A, F, T, P, rate, integration))
+        return set_error(BLADE_ERROR,
+                         "blade_beamform_detect_tc: unsupported configuration (B=%llu A=%llu T=%llu P=%llu rate=%llu "
+                         "I=%llu): needs P=2, 1<=A<=64, T%%128==0, rate in {1,2,4}, I a power of two <= 32",
+                         (unsigned long long)B, (unsigned long long)A, (unsigned long long)T, (unsigned long long)P,
+                         (unsigned long long)rate, (unsigned long long)integration);
+    if (!in || !plan || !out) return set_error(BLADE_ERROR, "blade_beamform_detect_tc: null buffer");
+    if (!aligned16(in) || !aligned16(plan) || (reinterpret_cast<uintptr_t>(out) & 3))
+        return set_error(BLADE_ERROR, "blade_beamform_detect_tc: input and plan must be 16-byte aligned");
+    return tc_run("blade_beamform_detect_tc", in, plan, out, B, A, F, T, rate, integration, 4,
+                  pick_kernel(rate, integration), stream);
+}
+
+extern "C" int blade_beamform_detect_tc_cf16(const void* in, const void* plan, void* out, uint64_t B, uint64_t A,
+                                             uint64_t F, uint64_t T, uint64_t P, uint64_t integration,
+                                             blade_stream_t stream) {
+    if (!blade_beamform_detect_tc_supported(B, A, F, T, P, 1, integration))
+        return set_error(BLADE_ERROR,
+                         "blade_beamform_detect_tc_cf16: unsupported configuration (B=%llu A=%llu T=%llu P=%llu "
+                         "I=%llu): needs P=2, 1<=A<=64, T%%128==0, I a power of two <= 32",
+                         (unsigned long long)B, (unsigned long long)A, (unsigned long long)T, (unsigned long long)P,
+                         (unsigned long long)integration);
+    if (!in || !plan || !out) return set_error(BLADE_ERROR, "blade_beamform_detect_tc_cf16: null buffer");
+    if (!aligned16(in) || !aligned16(plan) || (reinterpret_cast<uintptr_t>(out) & 3))
+        return set_error(BLADE_ERROR, "blade_beamform_detect_tc_cf16: input and plan must be 16-byte aligned");
+    return tc_run("blade_beamform_detect_tc_cf16", in, plan, out, B, A, F, T, 1, integration, 8,
+                  pick_cf16(integration), stream);
 }
 
 extern "C" int blade_device_status(uint32_t* status) {

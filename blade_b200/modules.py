@@ -689,8 +689,9 @@ class BeamformDetect(Module):
         self._output = self._alloc(self._shape, "f32")
         self._plan = None
         if prec == "fp16_split":
+            # the phasor image is rebuilt every step: one per Runner slot
             n = int(lib.blade_beamform_tc_plan_size(B, A, F, P))
-            self._plan = torch.empty(n, dtype=torch.uint8, device="cuda")
+            self._plan = self._alloc((n,), "i8", "tensor")
 
     def get_config(self):
         return self.config
@@ -711,9 +712,10 @@ class BeamformDetect(Module):
         R, I = int(self.config.rate), int(self.config.integration_size)
         s = _stream_handle(stream)
         if self.precision == "fp16_split":
-            _lib.call("blade_beamform_tc_prepare", ph.data_ptr(), self._plan.data_ptr(), B, A, F, P, s)
-            _lib.call("blade_beamform_detect_tc", buf.data_ptr(), self._plan.data_ptr(), out.data_ptr(), B, A, F, T,
-                      P, R, I, s)
+            plan = _out(self._plan)
+            _lib.call("blade_beamform_tc_prepare", ph.data_ptr(), plan.data_ptr(), B, A, F, P, s)
+            _lib.call("blade_beamform_detect_tc", buf.data_ptr(), plan.data_ptr(), out.data_ptr(), B, A, F, T, P, R,
+                      I, s)
         else:
             _lib.call("blade_beamform_detect_f32", type_code(buf.dtype), buf.data_ptr(), ph.data_ptr(),
                       out.data_ptr(), B, A, F, T, P, R, I, s)
@@ -800,6 +802,48 @@ class ModeH(Module):
         return result.success
 
 
+class _ModeBTensorCore(Module):
+    """ModeB on CI8 voltages with the detector (Stokes-I, no incoherent beam) at
+    channelizer rate 2 or 4: the pre-beamformer Cast -> Channelizer -> [Polarizer]
+    into an exact CF16 buffer (blade_prechannelize_cf16), then the per-fine-channel
+    phasor split and the tensor-core Beamformer -> Detector at rate 1
+    (blade_beamform_tc_prepare + blade_beamform_detect_tc_cf16).  Three launches."""
+
+    taint = Taint.CONSUMER | Taint.PRODUCER
+
+    def __init__(self, buffer, phasors, rate, integration, circular):
+        super().__init__()
+        self._buffer, self._phasors = buffer, phasors
+        self._R, self._I, self._circ = int(rate), int(integration), bool(circular)
+        A, F, T, P = as_vector(buffer).shape
+        B = as_vector(phasors).shape[0]
+        R = self._R
+        self._pre = self._alloc((A, F * R, T // R, P), "cf16")
+        n = int(_lib.load().blade_beamform_tc_plan_size(B, A, F * R, P))
+        self._plan = self._alloc((n,), "i8", "tensor")
+        self._output = self._alloc((B, F * R, T // (R * self._I), 1), "f32")
+
+    @staticmethod
+    def applies(it, A, F, T, P, B, R, I, detector, incoherent, OP) -> bool:
+        if it != "ci8" or not detector or incoherent or OP != 1 or P != 2 or R not in (2, 4) or T % R:
+            return False
+        return _lib.load().blade_beamform_detect_tc_supported(B, A, F * R, T // R, P, 1, I) == 1
+
+    def get_output(self):
+        return self._output
+
+    def process(self, step=0, stream=None):
+        x, ph = as_vector(self._buffer), as_vector(self._phasors)
+        pre, plan, out = _out(self._pre), _out(self._plan), _out(self._output)
+        A, F, T, P = x.shape
+        B, R, sh = ph.shape[0], self._R, _stream_handle(stream)
+        _lib.call("blade_prechannelize_cf16", x.data_ptr(), pre.data_ptr(), A, F, T, P, R, int(self._circ), sh)
+        _lib.call("blade_beamform_tc_prepare", ph.data_ptr(), plan.data_ptr(), B, A, F * R, P, sh)
+        _lib.call("blade_beamform_detect_tc_cf16", pre.data_ptr(), plan.data_ptr(), out.data_ptr(), B, A, F * R,
+                  T // R, P, self._I, sh)
+        return result.success
+
+
 class ModeB(Module):
     """Bundles::ATA::ModeB<IT, OT> (include/blade/bundles/ata/mode_b.hh:17-225, Python
     binding python/blade/ext_modeb.cc:20-114): Cast -> Channelizer (pre-beamformer,
@@ -816,8 +860,11 @@ class ModeB(Module):
     With the detector enabled the incoherent beam is square-rooted, as the bundle
     configures it (mode_b.hh:146-147).  When the chain is Beamformer -> Detector
     alone (rate 1, no circular conversion, no incoherent beam, Stokes-I), it runs
-    as one fused launch (tensor cores for CI8 input, FP32 CUDA cores for CF32);
-    every other configuration runs the module kernels in order."""
+    as one fused launch (tensor cores for CI8 input, FP32 CUDA cores for CF32).
+    CI8 input at rate 2 or 4 with Stokes-I and no incoherent beam runs the
+    pre-beamformer stages into exact FP16 and the tensor-core chain on the fine
+    channels (three launches, ``tensor_cores`` is True); every other
+    configuration runs the module kernels in order."""
 
     taint = Taint.CONSUMER | Taint.PRODUCER
 
@@ -893,7 +940,12 @@ class ModeB(Module):
         I, OP = int(c.detector_integration_size), int(c.detector_number_of_output_polarizations)
         self.fused = (c.detector_enable and R == 1 and not c.pre_beamformer_polarizer_convert_to_circular
                       and not c.beamformer_incoherent_beam and OP == 1 and P == 2 and I > 0 and T % I == 0)
-        if self.fused:
+        self.tensor_cores = (not self.fused) and _ModeBTensorCore.applies(
+            it, A, F, T, P, B, R, I, bool(c.detector_enable), bool(c.beamformer_incoherent_beam), OP)
+        if self.tensor_cores:
+            last = _ModeBTensorCore(input.buffer, phasors, R, I, c.pre_beamformer_polarizer_convert_to_circular)
+            self._stages.append(last)
+        elif self.fused:
             last = BeamformDetect(BeamformDetect.config(rate=1, integration_size=I, number_of_output_polarizations=1),
                                   BeamformDetect.input(buffer=input.buffer, phasors=phasors), it=it, ot="f32")
             self._stages.append(last)

@@ -236,6 +236,31 @@ BLADE_API int blade_beamform_detect_tc(const void* in, const void* plan, void* o
                              blade_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * ATA ModeB in the reference's own order (pre-beamformer channelizer, per fine
+ * channel phasors), as two launches:
+ *
+ * blade_prechannelize_cf16: Cast<CI8,CF32> -> Channelizer(rate) -> [Polarizer]
+ * of include/blade/bundles/ata/mode_b.hh:99-139 on CI8 [A,F,T,2] voltages, out
+ * CF16 [A, F*rate, T/rate, 2]: fftshifted rate-point DFT per spectrum
+ * (src/modules/channelizer/channelizer.cu:5-19 + cuFFT), then (X + iY, X - iY)
+ * when circular != 0 (src/modules/polarizer/polarizer.cu:17-23).  rate in
+ * {1, 2, 4}; every output value is an integer of magnitude <= 1024, exact in FP16
+ * (the CF32 module chain computes the same values).
+ *
+ * blade_beamform_detect_tc_cf16: the tensor-core Beamformer::ATA -> Detector
+ * (Stokes-I) chain of blade_beamform_detect_tc at rate 1 on CF16 [A,F,T,2]
+ * voltages (e.g. the output above, F counting fine channels) with the phasor
+ * image of blade_beamform_tc_prepare for [B,A,F,1,2] phasors; out F32
+ * [B,F,T/I,1].  Same shape limits as blade_beamform_detect_tc at rate 1.
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_prechannelize_cf16(const void* in, void* out, uint64_t A, uint64_t F,
+                             uint64_t T, uint64_t P, uint64_t rate, int circular,
+                             blade_stream_t stream);
+BLADE_API int blade_beamform_detect_tc_cf16(const void* in, const void* plan, void* out,
+                                  uint64_t B, uint64_t A, uint64_t F, uint64_t T,
+                                  uint64_t P, uint64_t integration, blade_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Device-side status of the pipelined kernels: every wait inside them is
  * bounded, and a wait that expires records a non-zero code here instead of
  * hanging (the kernel then drains its own work and returns).  Synchronous:
