@@ -10,7 +10,10 @@
 //    engine of Phasor::ATA (ERFA astrometry, src/modules/phasor/ata.cc:9-173) is
 //    not part of this library (blade_phasor_from_delays turns delays into phasors).
 //  * ModeB with the detector, rate 1, no circular conversion, no incoherent beam and
-//    Stokes-I is one fused launch (Modules::BeamformDetect: tensor cores for CI8).
+//    Stokes-I is one fused launch (Modules::BeamformDetect: tensor cores for CI8);
+//    with CI8 at rate 2 or 4 (Stokes-I, no incoherent beam) it runs the
+//    pre-beamformer stages into exact FP16 and the tensor-core chain on the fine
+//    channels (Modules::ModeBTensorCore).
 //  * ModeH at rate 65536 is one fused module (blade_spectrometer); other rates run
 //    the module chain Cast -> Channelizer -> Polarizer -> Detector -> Cast.
 #ifndef BLADE_B200_BUNDLES_HH
@@ -95,6 +98,63 @@ class Spectrometer : public Module {
     Vector<Device::CUDA, uint8_t, VectorShape> workspace;
 };
 
+// ModeB's pre-beamformer stages and beamformer + detector on tensor cores for CI8
+// voltages at rate 2 or 4 (Stokes-I, no incoherent beam): blade_prechannelize_cf16
+// into an exact CF16 buffer, then the per-fine-channel phasor split and
+// blade_beamform_detect_tc_cf16.
+class ModeBTensorCore : public Module {
+   public:
+    struct Config {
+        U64 rate = 4;
+        BOOL convertToCircular = false;
+        U64 integrationSize = 1;
+    };
+    struct Input {
+        const ArrayTensor<Device::CUDA, CI8>& buf;
+        const PhasorTensor<Device::CUDA, CF32>& phasors;
+    };
+
+    static bool applies(const ArrayShape& s, U64 B, U64 rate, U64 integration) {
+        return (rate == 2 || rate == 4) && s[3] == 2 && s[2] % rate == 0 &&
+               blade_beamform_detect_tc_supported(B, s[0], s[1] * rate, s[2] / rate, 2, 1, integration) == 1;
+    }
+
+    ModeBTensorCore(const Config& config, const Input& input, const Stream& = nullptr)
+        : config(config), input(input),
+          pre(ArrayShape({input.buf.shape()[0], input.buf.shape()[1] * config.rate,
+                          input.buf.shape()[2] / config.rate, 2})),
+          plan(VectorShape({blade_beamform_tc_plan_size(input.phasors.shape()[0], input.buf.shape()[0],
+                                                        input.buf.shape()[1] * config.rate, 2)})),
+          out(ArrayShape({input.phasors.shape()[0], input.buf.shape()[1] * config.rate,
+                          input.buf.shape()[2] / (config.rate * config.integrationSize), 1})) {}
+    const ArrayTensor<Device::CUDA, F32>& getOutputBuffer() const { return out.get(); }
+    Taint getTaint() const override { return Taint::CONSUMER | Taint::PRODUCER; }
+    std::string name() const override { return "ModeBTensorCore"; }
+    void setSlot(U64 i) override {
+        pre.set(i);
+        plan.set(i);
+        out.set(i);
+    }
+    Result process(const U64&, const Stream& stream = nullptr) override {
+        const auto& s = input.buf.shape();
+        const U64 B = input.phasors.shape()[0], R = config.rate;
+        int rc = blade_prechannelize_cf16(input.buf.data(), pre.get().data(), s[0], s[1], s[2], 2, R,
+                                          config.convertToCircular ? 1 : 0, stream);
+        if (!rc) rc = blade_beamform_tc_prepare(input.phasors.data(), plan.get().data(), B, s[0], s[1] * R, 2, stream);
+        if (!rc)
+            rc = blade_beamform_detect_tc_cf16(pre.get().data(), plan.get().data(), out.get().data(), B, s[0],
+                                               s[1] * R, s[2] / R, 2, config.integrationSize, stream);
+        return FromABI(rc);
+    }
+
+   private:
+    const Config config;
+    const Input input;
+    SlotOutput<ArrayTensor<Device::CUDA, CF16>> pre;
+    SlotOutput<Vector<Device::CUDA, uint8_t, VectorShape>> plan;
+    SlotOutput<ArrayTensor<Device::CUDA, F32>> out;
+};
+
 }  // namespace Modules
 
 namespace Bundles {
@@ -146,6 +206,18 @@ class ModeB : public Bundle {
                 checkOutput(beamformDetect->getOutputBuffer().shape());
                 return;
             }
+            if constexpr (std::is_same<IT, CI8>::value) {
+                if (config.detectorEnable && !config.beamformerIncoherentBeam &&
+                    config.detectorNumberOfOutputPolarizations == 1 &&
+                    Modules::ModeBTensorCore::applies(s, p[0], R, config.detectorIntegrationSize)) {
+                    this->connect(tensorCore, {.rate = R,
+                                               .convertToCircular = config.preBeamformerPolarizerConvertToCircular,
+                                               .integrationSize = config.detectorIntegrationSize},
+                                  {input.buffer, input.phasors});
+                    checkOutput(tensorCore->getOutputBuffer().shape());
+                    return;
+                }
+            }
         }
         const ArrayTensor<Device::CUDA, CF32>* x = nullptr;
         if constexpr (std::is_same<IT, CF32>::value) {
@@ -180,9 +252,11 @@ class ModeB : public Bundle {
     const Config& getConfig() const { return config; }
     const ArrayTensor<Device::CUDA, IT>& getInputBuffer() const { return input.buffer; }
     bool isFused() const { return fused; }
+    bool usesTensorCores() const { return tensorCore != nullptr; }
 
     const ArrayTensor<Device::CUDA, OT>& getOutputBuffer() const {
         if constexpr (std::is_same<OT, F32>::value) {
+            if (tensorCore) return tensorCore->getOutputBuffer();
             return fused ? beamformDetect->getOutputBuffer() : detector->getOutputBuffer();
         } else {
             return beamformer->getOutputBuffer();
@@ -204,6 +278,7 @@ class ModeB : public Bundle {
     std::shared_ptr<Modules::Beamformer::ATA<CF32, CF32>> beamformer;
     std::shared_ptr<Modules::Detector<CF32, F32>> detector;
     std::shared_ptr<Modules::BeamformDetect<IT, F32>> beamformDetect;
+    std::shared_ptr<Modules::ModeBTensorCore> tensorCore;
 };
 
 }  // namespace ATA

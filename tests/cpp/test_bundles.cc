@@ -52,13 +52,15 @@ static void phasors(PhasorTensor<Device::CUDA, CF32>& dev, uint32_t seed) {
 }
 
 template <typename Block, typename Out>
-static bool run(Pipeline& p, const std::string& dir, const std::string& name, const Out& out, bool fused) {
+static bool run(Pipeline& p, const std::string& dir, const std::string& name, const Out& out, bool fused,
+                bool tc = false) {
     if (p.compute(0) != Result::SUCCESS || p.synchronize(0) != Result::SUCCESS) {
         std::fprintf(stderr, "%s: compute failed: %s\n", name.c_str(), blade_last_error());
         return false;
     }
     if (!dump(dir + "/" + name + "_out.bin", out)) return false;
-    std::printf("{\"case\": \"%s\", \"fused\": %s}\n", name.c_str(), fused ? "true" : "false");
+    std::printf("{\"case\": \"%s\", \"fused\": %s, \"tc\": %s}\n", name.c_str(), fused ? "true" : "false",
+                tc ? "true" : "false");
     return true;
 }
 
@@ -85,7 +87,7 @@ static bool mode_b(const std::string& dir, const std::string& name, U64 A, U64 F
         return false;
     }
     if (!dump(dir + "/" + name + "_in.bin", in) || !dump(dir + "/" + name + "_ph.bin", ph)) return false;
-    return run<Bundle>(p, dir, name, b->getOutputBuffer(), b->isFused());
+    return run<Bundle>(p, dir, name, b->getOutputBuffer(), b->isFused(), b->usesTensorCores());
 }
 
 template <typename IT, typename OT>
@@ -138,6 +140,7 @@ int main(int argc, char** argv) {
     ok &= mode_b<CI8, F32>(dir, "modeb_ci8_r4", 12, 4, 512, 3, 4, true, true, true, 2, 1, 11);
     ok &= mode_b<CF32, F32>(dir, "modeb_cf32_r1", 20, 8, 512, 2, 1, false, false, true, 4, 1, 12);
     ok &= mode_b<CI8, CF32>(dir, "modeb_ci8_beams", 8, 4, 256, 2, 2, false, true, false, 1, 1, 13);
+    ok &= mode_b<CI8, F32>(dir, "modeb_ci8_r4_tc", 12, 4, 1024, 3, 4, true, false, true, 2, 1, 17);
     ok &= mode_h<CI8, F32>(dir, "modeh_ci8_65536", 1, 2, 65536, true, 1, 4, 14);
     ok &= mode_h<CF32, F32>(dir, "modeh_cf32_1024", 2, 3, 1024, false, 1, 1, 15);
     ok &= meerkat(dir, 16);

@@ -60,9 +60,11 @@ def test_cpp_bundles_match_oracle(cuda, tmp_path):
     exe = _compile(str(tmp_path / "test_bundles"), BUNDLES)
     r = subprocess.run([exe, str(tmp_path)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
-    fused = {d["case"]: d["fused"] for d in (json.loads(line) for line in r.stdout.strip().splitlines())}
-    assert fused == {"modeb_ci8_r4": False, "modeb_cf32_r1": True, "modeb_ci8_beams": False,
+    cases = [json.loads(line) for line in r.stdout.strip().splitlines()]
+    fused = {d["case"]: d["fused"] for d in cases}
+    assert fused == {"modeb_ci8_r4": False, "modeb_cf32_r1": True, "modeb_ci8_beams": False, "modeb_ci8_r4_tc": False,
                      "modeh_ci8_65536": True, "modeh_cf32_1024": False, "meerkat": False}
+    assert [d["case"] for d in cases if d["tc"]] == ["modeb_ci8_r4_tc"]
 
     def rel(a, b):
         return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
@@ -77,6 +79,11 @@ def test_cpp_bundles_match_oracle(cuda, tmp_path):
     x, w = ci8("modeb_ci8_r4", 12, 4, 512), _read(tmp_path / "modeb_ci8_r4_ph.bin", np.complex64, (3, 12, 16, 1, 2))
     got = _read(tmp_path / "modeb_ci8_r4_out.bin", np.float32, (4, 16, 64, 1))
     assert rel(got, O.mode_b(x, w, 4, True, True, True, 2, 1)) < 1e-5
+    # ModeB, CI8, rate 4, circular, no incoherent beam: the tensor-core path on the fine channels
+    x = ci8("modeb_ci8_r4_tc", 12, 4, 1024)
+    w = _read(tmp_path / "modeb_ci8_r4_tc_ph.bin", np.complex64, (3, 12, 16, 1, 2))
+    got = _read(tmp_path / "modeb_ci8_r4_tc_out.bin", np.float32, (3, 16, 128, 1))
+    assert rel(got, O.mode_b(x, w, 4, True, False, True, 2, 1)) < 1e-5
     # ModeB, CF32, rate 1, Stokes-I: the fused launch
     x, w = cf32("modeb_cf32_r1", 20, 8, 512), _read(tmp_path / "modeb_cf32_r1_ph.bin", np.complex64, (2, 20, 8, 1, 2))
     got = _read(tmp_path / "modeb_cf32_r1_out.bin", np.float32, (2, 8, 128, 1))
