@@ -21,8 +21,8 @@ block's launch latency eager against one CUDA graph (A = 20, F = 96, T = 256,
 B = 8; also as one fused FP32 launch and as the tensor-core pair), the forward +
 adjoint step of the Stokes loss (A = 28, B = 1, F = 192, T = 2048, CF32) and the
 ATA ModeB bundle in the reference's order on the production block
-(pre-beamformer channelizer, per-fine-channel phasors; tensor-core path, and the
-module chain with the incoherent beam);
+(pre-beamformer channelizer, per-fine-channel phasors; the tensor-core path with
+and without the incoherent beam, and the module chain);
 --skip-extra leaves them out.
 
 Multi-GPU (torchrun): weak scaling, every rank owns its own 192-channel band
@@ -479,12 +479,12 @@ def _measure_calls(fn, side, calls):
 def modeb_step(steps, warmup):
     """ATA ModeB in the reference's own order (include/blade/bundles/ata/mode_b.hh:99-199)
     on the production block: Cast -> Channelizer(rate 4) -> Beamformer with per-fine-
-    channel phasors -> Detector (Stokes-I, I=4), CI8 in, through bl.module(bl.modeb).
-    Without the incoherent beam (as the reference's ModeB test runs it) the bundle takes
-    the tensor-core path (pre-beamformer stages into exact FP16, then the tensor-core
-    chain on the 768 fine channels: three launches); with it, the module chain (five
-    launches)."""
+    channel phasors -> Detector (Stokes-I, I=4), CI8 in, through bl.module(bl.modeb):
+    the tensor-core path (pre-beamformer stages into exact FP16, the tensor-core chain
+    on the 768 fine channels, three launches; four with the incoherent beam), against
+    the same chain module by module (Cast, Channelizer, Beamformer, Detector)."""
     import blade_b200 as bl
+    from blade_b200.modules import BeamformerATA, Cast, Channelizer, Detector
 
     w = dict(WORK)
     A, F, T, P, B, R, I = (w[k] for k in ("A", "F", "T", "P", "B", "R", "I"))
@@ -495,6 +495,19 @@ def modeb_step(steps, warmup):
     ph.as_torch().copy_(torch.polar(torch.ones((B, A, F * R, 1, P), device="cuda"),
                                     torch.rand((B, A, F * R, 1, P), generator=g, device="cuda") * 6.283185307))
     s = torch.cuda.current_stream()
+
+    def timed(process):
+        for _ in range(warmup):
+            process()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(steps):
+            process()
+        e1.record(s)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
     res = {"workload": "A=28 F=192 T=8192 P=2 B=16, Cast->Channelizer(4)->Beamformer(fine phasors)"
                        "->Detector(Stokes-I, I=4)"}
     outs = {}
@@ -503,23 +516,24 @@ def modeb_step(steps, warmup):
                "pre_beamformer_channelizer_rate": R, "beamformer_incoherent_beam": inc, "detector_enable": True,
                "detector_integration_size": I, "detector_number_of_output_polarizations": 1}
         mod = bl.module(bl.modeb, cfg, {"buffer": buf, "phasors": ph}, it=bl.ci8, ot=bl.f32, telescope=bl.ata)
-        for _ in range(warmup):
-            mod.process(0, s)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(s)
-        for _ in range(steps):
-            mod.process(0, s)
-        e1.record(s)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / steps
+        ms = timed(lambda: mod.process(0, s))
         res[f"{label}path"] = "tensor cores" if mod.tensor_cores else "module chain"
         res[f"{label}ms_per_step"] = round(ms, 4)
         res[f"{label}tmacs"] = round(tmac(w) / (ms * 1e-3) / 1e12, 3)
-        outs[label] = mod.get_output().as_torch()[:B].clone()
+        outs[label] = mod.get_output().as_torch().clone()
         del mod
-    res["tc_vs_chain_rel_l2"] = float((outs[""] - outs["incoherent_"]).norm() / outs["incoherent_"].norm())
-    del buf, ph, outs
+    # the same block module by module (with the incoherent beam, square-rooted before the detector)
+    cast = Cast(Cast.config(), Cast.input(buf), it="ci8", ot="cf32")
+    chan = Channelizer(Channelizer.config(R), Channelizer.input(cast.get_output()))
+    bf = BeamformerATA(BeamformerATA.config(True, True), BeamformerATA.input(chan.get_output(), ph))
+    det = Detector(Detector.config(I, 1), Detector.input(bf.get_output()))
+    chain = [cast, chan, bf, det]
+    ms = timed(lambda: [m.process(0, s) for m in chain])
+    res["module_chain_ms_per_step"] = round(ms, 4)
+    res["module_chain_tmacs"] = round(tmac(w) / (ms * 1e-3) / 1e12, 3)
+    ref = det.get_output().as_torch()
+    res["tc_vs_module_chain_rel_l2"] = float((outs["incoherent_"] - ref).norm() / ref.norm())
+    del buf, ph, outs, chain, cast, chan, bf, det, ref
     return res
 
 

@@ -11,7 +11,7 @@
 //    not part of this library (blade_phasor_from_delays turns delays into phasors).
 //  * ModeB with the detector, rate 1, no circular conversion, no incoherent beam and
 //    Stokes-I is one fused launch (Modules::BeamformDetect: tensor cores for CI8);
-//    with CI8 at rate 2 or 4 (Stokes-I, no incoherent beam) it runs the
+//    with CI8 at rate 2 or 4 (Stokes-I) it runs the
 //    pre-beamformer stages into exact FP16 and the tensor-core chain on the fine
 //    channels (Modules::ModeBTensorCore).
 //  * ModeH at rate 65536 is one fused module (blade_spectrometer); other rates run
@@ -99,15 +99,17 @@ class Spectrometer : public Module {
 };
 
 // ModeB's pre-beamformer stages and beamformer + detector on tensor cores for CI8
-// voltages at rate 2 or 4 (Stokes-I, no incoherent beam): blade_prechannelize_cf16
-// into an exact CF16 buffer, then the per-fine-channel phasor split and
-// blade_beamform_detect_tc_cf16.
+// voltages at rate 2 or 4 (Stokes-I): blade_prechannelize_cf16 into an exact CF16
+// buffer, then the per-fine-channel phasor split and
+// blade_beamform_detect_tc_cf16, and with the incoherent beam its detected row
+// (blade_incoherent_detect_cf16).
 class ModeBTensorCore : public Module {
    public:
     struct Config {
         U64 rate = 4;
         BOOL convertToCircular = false;
         U64 integrationSize = 1;
+        BOOL incoherentBeam = false;
     };
     struct Input {
         const ArrayTensor<Device::CUDA, CI8>& buf;
@@ -125,7 +127,7 @@ class ModeBTensorCore : public Module {
                           input.buf.shape()[2] / config.rate, 2})),
           plan(VectorShape({blade_beamform_tc_plan_size(input.phasors.shape()[0], input.buf.shape()[0],
                                                         input.buf.shape()[1] * config.rate, 2)})),
-          out(ArrayShape({input.phasors.shape()[0], input.buf.shape()[1] * config.rate,
+          out(ArrayShape({input.phasors.shape()[0] + (config.incoherentBeam ? 1 : 0), input.buf.shape()[1] * config.rate,
                           input.buf.shape()[2] / (config.rate * config.integrationSize), 1})) {}
     const ArrayTensor<Device::CUDA, F32>& getOutputBuffer() const { return out.get(); }
     Taint getTaint() const override { return Taint::CONSUMER | Taint::PRODUCER; }
@@ -144,6 +146,10 @@ class ModeBTensorCore : public Module {
         if (!rc)
             rc = blade_beamform_detect_tc_cf16(pre.get().data(), plan.get().data(), out.get().data(), B, s[0],
                                                s[1] * R, s[2] / R, 2, config.integrationSize, stream);
+        if (!rc && config.incoherentBeam)  // beam row B
+            rc = blade_incoherent_detect_cf16(pre.get().data(), input.phasors.data(),
+                                              out.get().data() + B * s[1] * R * (s[2] / (R * config.integrationSize)),
+                                              s[0], s[1] * R, s[2] / R, 2, config.integrationSize, stream);
         return FromABI(rc);
     }
 
@@ -207,12 +213,12 @@ class ModeB : public Bundle {
                 return;
             }
             if constexpr (std::is_same<IT, CI8>::value) {
-                if (config.detectorEnable && !config.beamformerIncoherentBeam &&
-                    config.detectorNumberOfOutputPolarizations == 1 &&
+                if (config.detectorEnable && config.detectorNumberOfOutputPolarizations == 1 &&
                     Modules::ModeBTensorCore::applies(s, p[0], R, config.detectorIntegrationSize)) {
                     this->connect(tensorCore, {.rate = R,
                                                .convertToCircular = config.preBeamformerPolarizerConvertToCircular,
-                                               .integrationSize = config.detectorIntegrationSize},
+                                               .integrationSize = config.detectorIntegrationSize,
+                                               .incoherentBeam = config.beamformerIncoherentBeam},
                                   {input.buffer, input.phasors});
                     checkOutput(tensorCore->getOutputBuffer().shape());
                     return;

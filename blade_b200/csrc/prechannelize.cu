@@ -98,3 +98,62 @@ extern "C" int blade_prechannelize_cf16(const void* in, void* out, uint64_t A, u
     else launch_pre<4>(x, y, A * F, S, circular != 0, st);
     return check_launch("blade_prechannelize_cf16");
 }
+
+// ---- incoherent beam of ModeB with the detector, on the CF16 fine channels ----
+// Beamformer::ATA's incoherent beam (src/modules/beamformer/beamformer.cu:64-78:
+// sum_a |x * w[0]|^2 per polarisation, square-rooted when the detector follows,
+// mode_b.hh:146-147) followed by the Stokes-I detector (detector.cu:34-51), which
+// squares the root back: out[f, u] = sum_{t in window u} sum_p sum_a
+// |x[a,f,t,p]|^2 |w[0,a,f,0,p]|^2.  One thread per sample (coalesced 8-byte
+// loads), the window closed with lane shuffles; I is a power of two <= 32.
+namespace bb {
+namespace {
+
+__global__ void __launch_bounds__(256) incoherent_detect_cf16_kernel(const uint2* __restrict__ x,
+                                                                     const float2* __restrict__ w0, float* out,
+                                                                     uint32_t A, uint32_t F, uint32_t T, uint32_t I) {
+    extern __shared__ float g2[];  // |w[0, a, f, 0, p]|^2, [a][p]
+    const uint32_t f = blockIdx.y;
+    for (uint32_t i = threadIdx.x; i < 2 * A; i += blockDim.x) {
+        const float2 w = w0[((uint64_t)(i >> 1) * F + f) * 2 + (i & 1)];
+        g2[i] = w.x * w.x + w.y * w.y;
+    }
+    __syncthreads();
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    float acc = 0.f;
+    if (t < T) {
+        for (uint32_t a = 0; a < A; a++) {
+            const uint2 v = __ldg(x + ((uint64_t)a * F + f) * T + t);
+            const float2 p0 = __half22float2(*reinterpret_cast<const __half2*>(&v.x));
+            const float2 p1 = __half22float2(*reinterpret_cast<const __half2*>(&v.y));
+            acc = fmaf(p0.x * p0.x + p0.y * p0.y, g2[2 * a], acc);
+            acc = fmaf(p1.x * p1.x + p1.y * p1.y, g2[2 * a + 1], acc);
+        }
+    }
+    for (uint32_t off = 1; off < I; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (t < T && (t % I) == 0) out[(uint64_t)f * (T / I) + t / I] = acc;
+}
+
+}  // namespace
+}  // namespace bb
+
+extern "C" int blade_incoherent_detect_cf16(const void* in, const void* phasors, void* out, uint64_t A, uint64_t F,
+                                            uint64_t T, uint64_t P, uint64_t integration, blade_stream_t stream) {
+    using namespace bb;
+    if (P != 2) return set_error(BLADE_ERROR, "blade_incoherent_detect_cf16: P must be 2");
+    if (integration == 0 || integration > 32 || (integration & (integration - 1)) != 0 || T % integration != 0)
+        return set_error(BLADE_ERROR, "blade_incoherent_detect_cf16: integration must be a power of two <= 32 "
+                         "dividing T");
+    if (A * F * T == 0) return BLADE_SUCCESS;
+    if (F > 65535 || T >= (1ull << 31)) return set_error(BLADE_ERROR, "blade_incoherent_detect_cf16: too large");
+    if (!in || !phasors || !out) return set_error(BLADE_ERROR, "blade_incoherent_detect_cf16: null buffer");
+    if ((reinterpret_cast<uintptr_t>(in) & 7) || (reinterpret_cast<uintptr_t>(out) & 3))
+        return set_error(BLADE_ERROR, "blade_incoherent_detect_cf16: misaligned buffer");
+    const size_t smem = 2 * A * sizeof(float);
+    if (int rc = ensure_smem(reinterpret_cast<const void*>(incoherent_detect_cf16_kernel), smem)) return rc;
+    const dim3 grid((unsigned)((T + 255) / 256), (unsigned)F);
+    incoherent_detect_cf16_kernel<<<grid, 256, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
+        static_cast<const uint2*>(in), static_cast<const float2*>(phasors), static_cast<float*>(out), (uint32_t)A,
+        (uint32_t)F, (uint32_t)T, (uint32_t)integration);
+    return check_launch("blade_incoherent_detect_cf16");
+}

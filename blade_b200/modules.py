@@ -803,29 +803,30 @@ class ModeH(Module):
 
 
 class _ModeBTensorCore(Module):
-    """ModeB on CI8 voltages with the detector (Stokes-I, no incoherent beam) at
-    channelizer rate 2 or 4: the pre-beamformer Cast -> Channelizer -> [Polarizer]
-    into an exact CF16 buffer (blade_prechannelize_cf16), then the per-fine-channel
-    phasor split and the tensor-core Beamformer -> Detector at rate 1
-    (blade_beamform_tc_prepare + blade_beamform_detect_tc_cf16).  Three launches."""
+    """ModeB on CI8 voltages with the detector (Stokes-I) at channelizer rate 2 or 4:
+    the pre-beamformer Cast -> Channelizer -> [Polarizer] into an exact CF16 buffer
+    (blade_prechannelize_cf16), then the per-fine-channel phasor split and the
+    tensor-core Beamformer -> Detector at rate 1 (blade_beamform_tc_prepare +
+    blade_beamform_detect_tc_cf16), and with the incoherent beam its detected row
+    (blade_incoherent_detect_cf16).  Three or four launches."""
 
     taint = Taint.CONSUMER | Taint.PRODUCER
 
-    def __init__(self, buffer, phasors, rate, integration, circular):
+    def __init__(self, buffer, phasors, rate, integration, circular, incoherent=False):
         super().__init__()
         self._buffer, self._phasors = buffer, phasors
-        self._R, self._I, self._circ = int(rate), int(integration), bool(circular)
+        self._R, self._I, self._circ, self._inc = int(rate), int(integration), bool(circular), bool(incoherent)
         A, F, T, P = as_vector(buffer).shape
         B = as_vector(phasors).shape[0]
         R = self._R
         self._pre = self._alloc((A, F * R, T // R, P), "cf16")
         n = int(_lib.load().blade_beamform_tc_plan_size(B, A, F * R, P))
         self._plan = self._alloc((n,), "i8", "tensor")
-        self._output = self._alloc((B, F * R, T // (R * self._I), 1), "f32")
+        self._output = self._alloc((B + int(self._inc), F * R, T // (R * self._I), 1), "f32")
 
     @staticmethod
-    def applies(it, A, F, T, P, B, R, I, detector, incoherent, OP) -> bool:
-        if it != "ci8" or not detector or incoherent or OP != 1 or P != 2 or R not in (2, 4) or T % R:
+    def applies(it, A, F, T, P, B, R, I, detector, OP) -> bool:
+        if it != "ci8" or not detector or OP != 1 or P != 2 or R not in (2, 4) or T % R:
             return False
         return _lib.load().blade_beamform_detect_tc_supported(B, A, F * R, T // R, P, 1, I) == 1
 
@@ -841,6 +842,10 @@ class _ModeBTensorCore(Module):
         _lib.call("blade_beamform_tc_prepare", ph.data_ptr(), plan.data_ptr(), B, A, F * R, P, sh)
         _lib.call("blade_beamform_detect_tc_cf16", pre.data_ptr(), plan.data_ptr(), out.data_ptr(), B, A, F * R,
                   T // R, P, self._I, sh)
+        if self._inc:  # beam row B: the incoherent beam through the detector
+            row = out.data_ptr() + B * F * R * (T // (R * self._I)) * 4
+            _lib.call("blade_incoherent_detect_cf16", pre.data_ptr(), ph.data_ptr(), row, A, F * R, T // R, P,
+                      self._I, sh)
         return result.success
 
 
@@ -861,9 +866,9 @@ class ModeB(Module):
     configures it (mode_b.hh:146-147).  When the chain is Beamformer -> Detector
     alone (rate 1, no circular conversion, no incoherent beam, Stokes-I), it runs
     as one fused launch (tensor cores for CI8 input, FP32 CUDA cores for CF32).
-    CI8 input at rate 2 or 4 with Stokes-I and no incoherent beam runs the
-    pre-beamformer stages into exact FP16 and the tensor-core chain on the fine
-    channels (three launches, ``tensor_cores`` is True); every other
+    CI8 input at rate 2 or 4 with Stokes-I runs the pre-beamformer stages into
+    exact FP16 and the tensor-core chain on the fine channels, plus the detected
+    incoherent beam when enabled (``tensor_cores`` is True); every other
     configuration runs the module kernels in order."""
 
     taint = Taint.CONSUMER | Taint.PRODUCER
@@ -940,10 +945,11 @@ class ModeB(Module):
         I, OP = int(c.detector_integration_size), int(c.detector_number_of_output_polarizations)
         self.fused = (c.detector_enable and R == 1 and not c.pre_beamformer_polarizer_convert_to_circular
                       and not c.beamformer_incoherent_beam and OP == 1 and P == 2 and I > 0 and T % I == 0)
-        self.tensor_cores = (not self.fused) and _ModeBTensorCore.applies(
-            it, A, F, T, P, B, R, I, bool(c.detector_enable), bool(c.beamformer_incoherent_beam), OP)
+        self.tensor_cores = (not self.fused) and _ModeBTensorCore.applies(it, A, F, T, P, B, R, I,
+                                                                          bool(c.detector_enable), OP)
         if self.tensor_cores:
-            last = _ModeBTensorCore(input.buffer, phasors, R, I, c.pre_beamformer_polarizer_convert_to_circular)
+            last = _ModeBTensorCore(input.buffer, phasors, R, I, c.pre_beamformer_polarizer_convert_to_circular,
+                                    c.beamformer_incoherent_beam)
             self._stages.append(last)
         elif self.fused:
             last = BeamformDetect(BeamformDetect.config(rate=1, integration_size=I, number_of_output_polarizations=1),

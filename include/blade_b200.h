@@ -260,6 +260,16 @@ BLADE_API int blade_beamform_detect_tc_cf16(const void* in, const void* plan, vo
                                   uint64_t B, uint64_t A, uint64_t F, uint64_t T,
                                   uint64_t P, uint64_t integration, blade_stream_t stream);
 
+/* Incoherent beam of Beamformer::ATA (src/modules/beamformer/beamformer.cu:64-78,
+ * square-rooted because the detector follows, mode_b.hh:146-147) through the
+ * Stokes-I detector on CF16 [A,F,T,2] voltages: out[f, u] = sum over the window
+ * u of I samples, both polarisations and all antennas of |x|^2 |w[0,a,f,0,p]|^2
+ * (phasors CF32 [B,A,F,1,2], beam 0 used); out F32 [F, T/I] (beam row B of a
+ * ModeB output).  I a power of two <= 32. */
+BLADE_API int blade_incoherent_detect_cf16(const void* in, const void* phasors, void* out,
+                                 uint64_t A, uint64_t F, uint64_t T, uint64_t P,
+                                 uint64_t integration, blade_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Device-side status of the pipelined kernels: every wait inside them is
  * bounded, and a wait that expires records a non-zero code here instead of

@@ -64,7 +64,7 @@ def test_cpp_bundles_match_oracle(cuda, tmp_path):
     fused = {d["case"]: d["fused"] for d in cases}
     assert fused == {"modeb_ci8_r4": False, "modeb_cf32_r1": True, "modeb_ci8_beams": False, "modeb_ci8_r4_tc": False,
                      "modeh_ci8_65536": True, "modeh_cf32_1024": False, "meerkat": False}
-    assert [d["case"] for d in cases if d["tc"]] == ["modeb_ci8_r4_tc"]
+    assert [d["case"] for d in cases if d["tc"]] == ["modeb_ci8_r4", "modeb_ci8_r4_tc"]
 
     def rel(a, b):
         return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))

@@ -92,3 +92,36 @@ def test_modeb_module_takes_the_tensor_core_path(cuda):
     torch.cuda.synchronize()
     got = mod.get_output().as_torch().cpu().numpy()
     assert rel_l2(got, O.mode_b(xh, wh, R, True, False, True, I, 1)) < TOL
+
+
+@pytest.mark.parametrize("I", [1, 4, 32])
+def test_incoherent_detect_matches_oracle(cuda, I):
+    A, F, T, B, R = 10, 3, 512, 2, 4
+    xh, wh = ci8(A, F, T, 40 + I), phasors(B, A, F * R, 41)
+    wh = wh * np.linspace(0.5, 1.5, A)[None, :, None, None, None].astype(np.float32)  # unequal antenna gains
+    x, w = dev(xh), dev(wh)
+    y = pre(x, R, 1)
+    out = torch.empty((F * R, T // (R * I)), dtype=torch.float32, device="cuda")
+    call("blade_incoherent_detect_cf16", ptr(y), ptr(w), ptr(out), A, F * R, T // R, 2, I, stream())
+    ref = O.mode_b(xh, wh, R, True, True, True, I, 1)[B, :, :, 0]
+    assert rel_l2(host(out), ref) < TOL
+
+
+def test_modeb_module_tensor_cores_with_incoherent_beam(cuda):
+    A, F, T, B, R, I = 8, 4, 1024, 2, 2, 4
+    xh, wh = ci8(A, F, T, 90), phasors(B, A, F * R, 91)
+    buf = bl.array_tensor((A, F, T, 2), dtype=bl.ci8, device=bl.cuda)
+    buf.as_torch().copy_(dev(xh))
+    ph = bl.phasor_tensor((B, A, F * R, 1, 2), dtype=bl.cf32, device=bl.cuda)
+    ph.as_torch().copy_(dev(wh))
+    cfg = {"input_shape": (A, F, T, 2), "output_shape": (B + 1, F * R, T // (R * I), 1),
+           "pre_beamformer_channelizer_rate": R, "beamformer_incoherent_beam": True, "detector_enable": True,
+           "detector_integration_size": I, "detector_number_of_output_polarizations": 1}
+    mod = bl.module(bl.modeb, cfg, {"buffer": buf, "phasors": ph}, it=bl.ci8, ot=bl.f32, telescope=bl.ata)
+    assert mod.tensor_cores
+    mod.process()
+    torch.cuda.synchronize()
+    got = mod.get_output().as_torch().cpu().numpy()
+    ref = O.mode_b(xh, wh, R, False, True, True, I, 1)
+    assert rel_l2(got[:B], ref[:B]) < TOL
+    assert rel_l2(got[B], ref[B]) < TOL
