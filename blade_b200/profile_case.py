@@ -7,7 +7,9 @@ Workloads: ata-small (A=20 F=96 T=256 B=8 rate 1 I=4), ata-production
 I=8), spectrometer (A=1 F=64 T=2^20, rate 65536, I=8, no beamformer) and
 spectrometer-small (the same with F=16, for full profiler captures), calibration
 (A=28 F=192 T=2048 B=1, CF32 voltages; path adjoint: the Stokes loss and its
-gradient).  Paths: tc
+gradient), modeb (the ATA production block through ModeB in the reference's
+order: CF16 pre-channelizer, then the CF16 tensor-core chain on 768 fine
+channels).  Paths: tc
 (phasor split + tensor-core chain), f32 (fused FP32 chain), modules (Cast ->
 Beamformer -> Channelizer -> Detector, one launch each; for the spectrometer
 Cast -> Channelizer -> Polarizer -> Detector; path fused: blade_spectrometer).
@@ -30,6 +32,7 @@ WORKLOADS = {
     "spectrometer": dict(A=1, F=64, T=1 << 20, B=0, R=65536, I=8),
     "spectrometer-small": dict(A=1, F=16, T=1 << 20, B=0, R=65536, I=8),
     "calibration": dict(A=28, F=192, T=2048, B=1, R=1, I=1),
+    "modeb": dict(A=28, F=192, T=8192, B=16, R=4, I=4),
 }
 
 
@@ -45,6 +48,23 @@ def main():
     s = torch.cuda.current_stream().cuda_stream
     g = torch.Generator(device="cuda").manual_seed(7)
     x = (torch.randn((A, F, T, P, 2), generator=g, device="cuda") * 8).round_().clamp_(-127, 127).to(torch.int8)
+    if args.workload == "modeb":
+        # ModeB in the reference's order on tensor cores: CF16 fine channels, then
+        # the per-fine-channel phasor split and the CF16 tensor-core chain
+        FR, TR = F * R, T // R
+        pre = torch.empty((A, FR, TR, P, 2), dtype=torch.float16, device="cuda")
+        ph = torch.polar(torch.ones((B, A, FR, 1, P), device="cuda"),
+                         torch.rand((B, A, FR, 1, P), generator=g, device="cuda") * 6.283185307)
+        plan = torch.empty(int(lib.blade_beamform_tc_plan_size(B, A, FR, P)), dtype=torch.uint8, device="cuda")
+        out = torch.empty((B, FR, TR // I, 1), dtype=torch.float32, device="cuda")
+        for _ in range(args.launches):
+            _lib.call("blade_prechannelize_cf16", x.data_ptr(), pre.data_ptr(), A, F, T, P, R, 0, s)
+            _lib.call("blade_beamform_tc_prepare", ph.data_ptr(), plan.data_ptr(), B, A, FR, P, s)
+            _lib.call("blade_beamform_detect_tc_cf16", pre.data_ptr(), plan.data_ptr(), out.data_ptr(), B, A, FR, TR,
+                      P, I, s)
+        torch.cuda.synchronize()
+        print(f"modeb tc: {args.launches} launches ok")
+        return
     if args.path == "adjoint":
         xc = torch.complex(torch.randn((A, F, T, P), generator=g, device="cuda"),
                            torch.randn((A, F, T, P), generator=g, device="cuda"))
