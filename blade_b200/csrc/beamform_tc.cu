@@ -359,6 +359,42 @@ __device__ __forceinline__ void build_operand_h16(const uint8_t* raw, uint32_t r
     }
 }
 
+// Both polarisations of one CF16 tile in one pass: one 8-byte load per (antenna,
+// sample) feeds both operands (consecutive lanes read consecutive 8-byte samples,
+// so a warp's loads are conflict-free).
+__device__ __forceinline__ void build_operand_h16_pair(const uint8_t* raw, uint32_t rrow, uint8_t* op0, uint8_t* op1,
+                                                       uint32_t A, uint32_t KA, uint32_t ct) {
+    constexpr uint32_t kStride = kConvWarps * 32;
+    const uint32_t ntasks = kM * (KA / 8);
+    for (uint32_t t = ct; t < ntasks; t += kStride) {
+        const uint32_t s = t % kM, g = t / kM;
+        uint2 v[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const uint32_t a = g * 8 + i;
+            v[i] = a < A ? *reinterpret_cast<const uint2*>(raw + a * rrow + s * 8) : make_uint2(0u, 0u);
+        }
+#pragma unroll
+        for (int p = 0; p < 2; p++) {
+            uint32_t h[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) h[i] = p ? v[i].y : v[i].x;
+            uint4 vr, vi;
+            vr.x = __byte_perm(h[0], h[1], 0x5410);
+            vr.y = __byte_perm(h[2], h[3], 0x5410);
+            vr.z = __byte_perm(h[4], h[5], 0x5410);
+            vr.w = __byte_perm(h[6], h[7], 0x5410);
+            vi.x = __byte_perm(h[0], h[1], 0x7632);
+            vi.y = __byte_perm(h[2], h[3], 0x7632);
+            vi.z = __byte_perm(h[4], h[5], 0x7632);
+            vi.w = __byte_perm(h[6], h[7], 0x7632);
+            uint8_t* op = p ? op1 : op0;
+            *reinterpret_cast<uint4*>(op + op_off(s, g * 8)) = vr;
+            *reinterpret_cast<uint4*>(op + op_off(s, KA + g * 8)) = vi;
+        }
+    }
+}
+
 // Both polarisations of one tile for R = 1 and 2: two single-polarisation passes.
 template <int R>
 __device__ __forceinline__ void build_operand_pair(const uint8_t* raw, uint32_t rrow, uint8_t* op0, uint8_t* op1, uint32_t A,
@@ -809,8 +845,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
                     for (uint32_t i = 0; i < kMaxT4; i++)
                         if (i < nt4) r4_pair_task(raw, g.raw_row, op0, op1, t4[i]);
                 } else if constexpr (ES == 8) {
-                    build_operand_h16(raw, g.raw_row, op0, g.A, KA, 0, ct);
-                    build_operand_h16(raw, g.raw_row, op1, g.A, KA, 1, ct);
+                    build_operand_h16_pair(raw, g.raw_row, op0, op1, g.A, KA, ct);
                 } else {
                     build_operand_pair<R>(raw, g.raw_row, op0, op1, g.A, KA, ct);
                 }

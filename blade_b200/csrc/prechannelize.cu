@@ -22,9 +22,25 @@ __global__ void __launch_bounds__(256) prechannelize_kernel(const uint32_t* __re
         const uint64_t af = i / S;
         const uint32_t s = (uint32_t)(i - af * S);
         float xr[2][R], xi[2][R];
+        // the spectrum's R sample words in one aligned 4R-byte load
+        uint32_t ws[R];
+        const uint32_t* src = in + af * (uint64_t)S * R + (uint64_t)s * R;
+        if constexpr (R == 4) {
+            const uint4 v = __ldg(reinterpret_cast<const uint4*>(src));
+            ws[0] = v.x;
+            ws[1 % R] = v.y;
+            ws[2 % R] = v.z;
+            ws[3 % R] = v.w;
+        } else if constexpr (R == 2) {
+            const uint2 v = __ldg(reinterpret_cast<const uint2*>(src));
+            ws[0] = v.x;
+            ws[1 % R] = v.y;
+        } else {
+            ws[0] = __ldg(src);
+        }
 #pragma unroll
         for (int j = 0; j < R; j++) {
-            const uint32_t w = __ldg(in + af * (uint64_t)S * R + (uint64_t)s * R + j);
+            const uint32_t w = ws[j];
             const float sg = (j & 1) ? -1.f : 1.f;  // fftshift pre-multiply (even R)
             xr[0][j] = (R > 1 ? sg : 1.f) * (float)(int8_t)(w & 0xFFu);
             xi[0][j] = (R > 1 ? sg : 1.f) * (float)(int8_t)((w >> 8) & 0xFFu);
@@ -87,8 +103,9 @@ extern "C" int blade_prechannelize_cf16(const void* in, void* out, uint64_t A, u
     if (T / rate > 0xFFFFFFFFull) return set_error(BLADE_ERROR, "blade_prechannelize_cf16: T too large");
     if (A * F * T == 0) return BLADE_SUCCESS;
     if (!in || !out) return set_error(BLADE_ERROR, "blade_prechannelize_cf16: null buffer");
-    if ((reinterpret_cast<uintptr_t>(in) & 3) || (reinterpret_cast<uintptr_t>(out) & 7))
-        return set_error(BLADE_ERROR, "blade_prechannelize_cf16: input must be 4-byte and output 8-byte aligned");
+    if ((reinterpret_cast<uintptr_t>(in) & (4 * rate - 1)) || (reinterpret_cast<uintptr_t>(out) & 7))
+        return set_error(BLADE_ERROR, "blade_prechannelize_cf16: input must be (4 x rate)-byte and output 8-byte "
+                         "aligned");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const uint32_t* x = static_cast<const uint32_t*>(in);
     uint2* y = static_cast<uint2*>(out);
