@@ -90,14 +90,6 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int x, 
         : "memory");
 }
 
-// L2 prefetch of the same 3-D box (no shared memory, no completion signal).
-__device__ __forceinline__ void tma_prefetch_3d(const void* tmap, int x, int y, int z) {
-    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
-                     reinterpret_cast<uint64_t>(tmap)),
-                 "r"(x), "r"(y), "r"(z)
-                 : "memory");
-}
-
 __device__ __forceinline__ void fence_proxy_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
