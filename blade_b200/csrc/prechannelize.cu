@@ -13,69 +13,91 @@ namespace bb {
 namespace {
 
 // One thread per (a, f, spectrum s): R sample words in, R dual-polarisation
-// CF16 samples out (8 bytes each, consecutive threads write consecutive s).
+// CF16 samples out (8 bytes each, consecutive threads write consecutive s).  Each
+// thread keeps the loads of kSpt spectra in flight before it computes any of them.
+constexpr int kSpt = 4;
+
+template <int R>
+__device__ __forceinline__ void load_spectrum(const uint32_t* src, uint32_t (&ws)[R]) {
+    if constexpr (R == 4) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(src));
+        ws[0] = v.x;
+        ws[1 % R] = v.y;
+        ws[2 % R] = v.z;
+        ws[3 % R] = v.w;
+    } else if constexpr (R == 2) {
+        const uint2 v = __ldg(reinterpret_cast<const uint2*>(src));
+        ws[0] = v.x;
+        ws[1 % R] = v.y;
+    } else {
+        ws[0] = __ldg(src);
+    }
+}
+
+template <int R, bool CIRC>
+__device__ __forceinline__ void spectrum_out(const uint32_t (&ws)[R], uint2* __restrict__ out, uint64_t af,
+                                             uint32_t S, uint32_t s) {
+    float xr[2][R], xi[2][R];
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        const uint32_t w = ws[j];
+        const float sg = (R > 1 && (j & 1)) ? -1.f : 1.f;  // fftshift pre-multiply (even R)
+        xr[0][j] = sg * (float)(int8_t)(w & 0xFFu);
+        xi[0][j] = sg * (float)(int8_t)((w >> 8) & 0xFFu);
+        xr[1][j] = sg * (float)(int8_t)((w >> 16) & 0xFFu);
+        xi[1][j] = sg * (float)(int8_t)(w >> 24);
+    }
+#pragma unroll
+    for (int k = 0; k < R; k++) {
+        float zr[2], zi[2];
+#pragma unroll
+        for (int p = 0; p < 2; p++) {
+            zr[p] = 0.f;
+            zi[p] = 0.f;
+#pragma unroll
+            for (int j = 0; j < R; j++) {
+                // e^{-2 pi i j k / R} for R <= 4 is one of 1, -i, -1, i
+                const int q = (j * k * (4 / R)) & 3;
+                const float re = xr[p][j], im = xi[p][j];
+                zr[p] += q == 0 ? re : q == 1 ? im : q == 2 ? -re : -im;
+                zi[p] += q == 0 ? im : q == 1 ? -re : q == 2 ? -im : re;
+            }
+        }
+        if (CIRC) {
+            const float lr = zr[0] - zi[1], li = zi[0] + zr[1];  // X + iY
+            const float rr = zr[0] + zi[1], ri = zi[0] - zr[1];  // X - iY
+            zr[0] = lr;
+            zi[0] = li;
+            zr[1] = rr;
+            zi[1] = ri;
+        }
+        const __half2 h0 = __floats2half2_rn(zr[0], zi[0]), h1 = __floats2half2_rn(zr[1], zi[1]);
+        uint2 o;
+        o.x = *reinterpret_cast<const uint32_t*>(&h0);
+        o.y = *reinterpret_cast<const uint32_t*>(&h1);
+        out[(af * R + k) * (uint64_t)S + s] = o;
+    }
+}
+
 template <int R, bool CIRC>
 __global__ void __launch_bounds__(256) prechannelize_kernel(const uint32_t* __restrict__ in,
                                                             uint2* __restrict__ out, uint64_t AF, uint32_t S) {
     const uint64_t n = AF * S;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t af = i / S;
-        const uint32_t s = (uint32_t)(i - af * S);
-        float xr[2][R], xi[2][R];
-        // the spectrum's R sample words in one aligned 4R-byte load
-        uint32_t ws[R];
-        const uint32_t* src = in + af * (uint64_t)S * R + (uint64_t)s * R;
-        if constexpr (R == 4) {
-            const uint4 v = __ldg(reinterpret_cast<const uint4*>(src));
-            ws[0] = v.x;
-            ws[1 % R] = v.y;
-            ws[2 % R] = v.z;
-            ws[3 % R] = v.w;
-        } else if constexpr (R == 2) {
-            const uint2 v = __ldg(reinterpret_cast<const uint2*>(src));
-            ws[0] = v.x;
-            ws[1 % R] = v.y;
-        } else {
-            ws[0] = __ldg(src);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; base < n; base += kSpt * stride) {
+        uint32_t ws[kSpt][R];
+#pragma unroll
+        for (int q = 0; q < kSpt; q++) {
+            const uint64_t i = base + q * stride;
+            if (i < n) load_spectrum<R>(in + i * R, ws[q]);  // spectrum i = af * S + s starts at word i * R
         }
 #pragma unroll
-        for (int j = 0; j < R; j++) {
-            const uint32_t w = ws[j];
-            const float sg = (j & 1) ? -1.f : 1.f;  // fftshift pre-multiply (even R)
-            xr[0][j] = (R > 1 ? sg : 1.f) * (float)(int8_t)(w & 0xFFu);
-            xi[0][j] = (R > 1 ? sg : 1.f) * (float)(int8_t)((w >> 8) & 0xFFu);
-            xr[1][j] = (R > 1 ? sg : 1.f) * (float)(int8_t)((w >> 16) & 0xFFu);
-            xi[1][j] = (R > 1 ? sg : 1.f) * (float)(int8_t)(w >> 24);
-        }
-#pragma unroll
-        for (int k = 0; k < R; k++) {
-            float zr[2], zi[2];
-#pragma unroll
-            for (int p = 0; p < 2; p++) {
-                zr[p] = 0.f;
-                zi[p] = 0.f;
-#pragma unroll
-                for (int j = 0; j < R; j++) {
-                    // e^{-2 pi i j k / R} for R <= 4 is one of 1, -i, -1, i
-                    const int q = (j * k * (4 / R)) & 3;
-                    const float re = xr[p][j], im = xi[p][j];
-                    zr[p] += q == 0 ? re : q == 1 ? im : q == 2 ? -re : -im;
-                    zi[p] += q == 0 ? im : q == 1 ? -re : q == 2 ? -im : re;
-                }
+        for (int q = 0; q < kSpt; q++) {
+            const uint64_t i = base + q * stride;
+            if (i < n) {
+                const uint64_t af = i / S;
+                spectrum_out<R, CIRC>(ws[q], out, af, S, (uint32_t)(i - af * S));
             }
-            if (CIRC) {
-                const float lr = zr[0] - zi[1], li = zi[0] + zr[1];  // X + iY
-                const float rr = zr[0] + zi[1], ri = zi[0] - zr[1];  // X - iY
-                zr[0] = lr;
-                zi[0] = li;
-                zr[1] = rr;
-                zi[1] = ri;
-            }
-            const __half2 h0 = __floats2half2_rn(zr[0], zi[0]), h1 = __floats2half2_rn(zr[1], zi[1]);
-            uint2 o;
-            o.x = *reinterpret_cast<const uint32_t*>(&h0);
-            o.y = *reinterpret_cast<const uint32_t*>(&h1);
-            out[(af * R + k) * (uint64_t)S + s] = o;
         }
     }
 }
