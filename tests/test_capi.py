@@ -117,3 +117,24 @@ def test_spectrometer_validation():
     for (it, ot, A, F, T, P, rate, I, OP), word in bad:
         st, msg = _err("blade_spectrometer", it, None, ot, None, None, A, F, T, P, rate, I, OP, 0, None)
         assert st == _lib.ERROR and word in msg, (word, msg)
+
+
+def test_modeb_tensor_core_entry_points_validate_on_the_host():
+    # rate, T % rate, P and integration checks return before any device work
+    for args, word in [((1, 1, 64, 2, 8, 0), "rate"), ((1, 1, 63, 2, 2, 0), "divisible"), ((1, 1, 64, 1, 2, 0), "P")]:
+        st, msg = _err("blade_prechannelize_cf16", None, None, *args, None)
+        assert st == _lib.ERROR and word in msg, (word, msg)
+    st, msg = _err("blade_beamform_detect_tc_cf16", None, None, None, 16, 28, 4, 100, 2, 4, None)
+    assert st == _lib.ERROR and "unsupported" in msg  # T % 128
+    st, msg = _err("blade_beamform_detect_tc_cf16", None, None, None, 16, 28, 4, 128, 2, 3, None)
+    assert st == _lib.ERROR and "unsupported" in msg  # I not a power of two
+    for args, word in [((4, 2, 64, 1, 4), "P"), ((4, 2, 64, 2, 3), "integration"), ((4, 2, 64, 2, 64), "integration")]:
+        st, msg = _err("blade_incoherent_detect_cf16", None, None, None, *args, None)
+        assert st == _lib.ERROR and word in msg, (word, msg)
+
+
+def test_meerkat_validation():
+    st, msg = _err("blade_beamform_meerkat_f32", None, None, None, 2, 4, 3, 16, 3, 0, None)
+    assert st == _lib.ERROR and "P must be" in msg
+    st, msg = _err("blade_beamform_meerkat_f32", None, None, None, 2, 4, 3, 16, 2, 0, None)
+    assert st == _lib.ERROR and "null" in msg
