@@ -94,3 +94,17 @@ def test_result_soft_bit():
         assert int(r) & (1 << 4)
     for r in (bl.result.error, bl.result.cuda_error, bl.result.assertion_error):
         assert not int(r) & (1 << 4)
+
+
+def test_modeb_tensor_core_dispatch():
+    # which ModeB configurations take the tensor-core path (host logic, no GPU)
+    from blade_b200.modules import _ModeBTensorCore as M
+
+    assert M.applies("ci8", 28, 192, 8192, 2, 16, 4, 4, True, 1)
+    assert M.applies("ci8", 64, 4, 1024, 2, 200, 2, 32, True, 1)      # several 64-beam chunks
+    assert not M.applies("cf32", 28, 192, 8192, 2, 16, 4, 4, True, 1)  # CF32 voltages: module chain
+    assert not M.applies("ci8", 28, 192, 8192, 2, 16, 8, 4, True, 1)   # rate 8: module chain
+    assert not M.applies("ci8", 28, 192, 8192, 2, 16, 4, 4, False, 1)  # no detector: beams out
+    assert not M.applies("ci8", 28, 192, 8192, 2, 16, 4, 4, True, 4)   # four products
+    assert not M.applies("ci8", 28, 192, 256, 2, 16, 4, 1, True, 1)    # 64 spectra: not a 128-row tile
+    assert not M.applies("ci8", 65, 4, 1024, 2, 16, 4, 1, True, 1)     # more than 64 antennas
