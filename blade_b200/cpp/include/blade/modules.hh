@@ -400,10 +400,9 @@ class BeamformDetect : public Module {
         const auto& s = input.buf.shape();
         const U64 B = input.phasors.shape()[0];
         if (tc) {
-            int rc = blade_beamform_tc_prepare(input.phasors.data(), plan.data(), B, s[0], s[1], s[3], stream);
-            if (rc) return FromABI(rc);
-            return FromABI(blade_beamform_detect_tc(input.buf.data(), plan.data(), out.get().data(), B, s[0], s[1],
-                                                    s[2], s[3], config.rate, config.integrationSize, stream));
+            return FromABI(blade_beamform_prepare_detect_tc(input.phasors.data(), plan.data(), input.buf.data(),
+                                                            out.get().data(), B, s[0], s[1], s[2], s[3], config.rate,
+                                                            config.integrationSize, stream));
         }
         return FromABI(blade_beamform_detect_f32(TypeInfo<IT>::code, input.buf.data(), input.phasors.data(),
                                                  out.get().data(), B, s[0], s[1], s[2], s[3], config.rate,

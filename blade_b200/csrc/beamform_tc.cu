@@ -85,6 +85,7 @@ struct TcArgs {
     uint32_t img_bytes, raw_bytes, tiles_per_ch;
     uint32_t raw_tiles, raw_row;  // tiles per raw stage (1, 2 or 4) and its antenna row stride (raw_tiles * 512)
     uint64_t total_tiles;
+    uint32_t pdl;  // launched as a programmatic dependent of the phasor split: wait for it before the image
 };
 
 __device__ __forceinline__ uint32_t cvt_pair(uint32_t v) {
@@ -653,6 +654,9 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
                 int ok = 1;
                 if (L == L0 || tt == 0) {
                     if (lane == 0) {
+                        // the phasor image is the preceding grid's output: with a programmatic
+                        // launch, everything above overlapped that grid, and here it must be done
+                        if (g.pdl && L == L0) asm volatile("griddepcontrol.wait;" ::: "memory");
                         ok = mbar_wait(w_empty, wph ^ 1, abort, kWaitBudget);
                         if (ok) {
                             mbar_arrive_expect_tx(w_full, g.img_bytes);
@@ -914,6 +918,9 @@ __global__ void __launch_bounds__(256) tc_prepare_kernel(const float2* __restric
                                                          uint32_t B, uint32_t A, uint32_t F, uint32_t NB,
                                                          uint32_t KA, uint32_t nchunks, uint32_t img_bytes,
                                                          uint32_t stacked) {
+    // a chain kernel launched as this grid's programmatic dependent may start its
+    // prologue now; it waits for this grid to finish before it reads the image
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const uint32_t groups = KA / 8;
     const uint32_t n = nchunks * F * 2u * NB * groups;
     const uint32_t ph_bytes = (KA == 64 ? 3u : 2u) * NB * 128u;
@@ -1157,7 +1164,8 @@ namespace {
 
 // Launches the chain over the 64-beam chunks once the arguments are checked.
 int tc_run(const char* who, const void* in, const void* plan, void* out, uint64_t B, uint64_t A, uint64_t F,
-           uint64_t T, uint64_t rate, uint64_t integration, uint32_t es, TcKernel fn, blade_stream_t stream) {
+           uint64_t T, uint64_t rate, uint64_t integration, uint32_t es, TcKernel fn, blade_stream_t stream,
+           bool pdl = false) {
     TcShape s;
     tc_shape(B, A, s, T, es);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
@@ -1187,12 +1195,30 @@ int tc_run(const char* who, const void* in, const void* plan, void* out, uint64_
         g.stacked = s.stacked;
         g.tiles_per_ch = (uint32_t)(T / kM);
         g.total_tiles = (uint64_t)F * (T / kM);
+        g.pdl = (pdl && c == 0) ? 1u : 0u;
         // Whole raw stages per CTA (the kernel rounds its share up to raw_tiles); no
         // CTA is left without tiles.
         const uint64_t sms = (uint64_t)sm_count();
         const uint64_t per = ((g.total_tiles + sms - 1) / sms + s.raw_tiles - 1) / s.raw_tiles * s.raw_tiles;
         const uint64_t grid = (g.total_tiles + per - 1) / per;
-        fn<<<(unsigned)grid, kThreads, s.smem, st>>>(g, tmap);
+        if (g.pdl) {
+            // programmatic dependent of the phasor split launched just before on this
+            // stream: prologue and raw loads overlap it (the kernel waits before the image)
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)grid, 1, 1);
+            cfg.blockDim = dim3(kThreads, 1, 1);
+            cfg.dynamicSmemBytes = s.smem;
+            cfg.stream = st;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attr[0].val.programmaticStreamSerializationAllowed = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            const cudaError_t e = cudaLaunchKernelEx(&cfg, fn, g, tmap);
+            if (e != cudaSuccess) return check_cuda(e, who);
+        } else {
+            fn<<<(unsigned)grid, kThreads, s.smem, st>>>(g, tmap);
+        }
         if (int rc = check_launch(who)) return rc;
     }
     return BLADE_SUCCESS;
@@ -1228,6 +1254,24 @@ extern "C" int blade_beamform_detect_tc(const void* in, const void* plan, void* 
         return set_error(BLADE_ERROR, "blade_beamform_detect_tc: input and plan must be 16-byte aligned");
     return tc_run("blade_beamform_detect_tc", in, plan, out, B, A, F, T, rate, integration, 4,
                   pick_kernel(rate, integration), stream);
+}
+
+extern "C" int blade_beamform_prepare_detect_tc(const void* phasors, void* plan, const void* in, void* out,
+                                                uint64_t B, uint64_t A, uint64_t F, uint64_t T, uint64_t P,
+                                                uint64_t rate, uint64_t integration, blade_stream_t stream) {
+    if (!blade_beamform_detect_tc_supported(B, A, F, T, P, rate, integration))
+        return set_error(BLADE_ERROR,
+                         "blade_beamform_prepare_detect_tc: unsupported configuration (B=%llu A=%llu T=%llu P=%llu "
+                         "rate=%llu I=%llu): needs P=2, 1<=A<=64, T%%128==0, rate in {1,2,4}, I a power of two <= 32",
+                         (unsigned long long)B, (unsigned long long)A, (unsigned long long)T, (unsigned long long)P,
+                         (unsigned long long)rate, (unsigned long long)integration);
+    if (!in || !plan || !out || !phasors) return set_error(BLADE_ERROR, "blade_beamform_prepare_detect_tc: null buffer");
+    if (!aligned16(in) || !aligned16(plan) || (reinterpret_cast<uintptr_t>(out) & 3))
+        return set_error(BLADE_ERROR, "blade_beamform_prepare_detect_tc: input and plan must be 16-byte aligned");
+    if (F == 0) return BLADE_SUCCESS;  // no split launched: nothing may follow it programmatically
+    if (int rc = blade_beamform_tc_prepare(phasors, plan, B, A, F, P, stream)) return rc;
+    return tc_run("blade_beamform_prepare_detect_tc", in, plan, out, B, A, F, T, rate, integration, 4,
+                  pick_kernel(rate, integration), stream, true);
 }
 
 extern "C" int blade_beamform_detect_tc_cf16(const void* in, const void* plan, void* out, uint64_t B, uint64_t A,

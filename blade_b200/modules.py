@@ -713,9 +713,8 @@ class BeamformDetect(Module):
         s = _stream_handle(stream)
         if self.precision == "fp16_split":
             plan = _out(self._plan)
-            _lib.call("blade_beamform_tc_prepare", ph.data_ptr(), plan.data_ptr(), B, A, F, P, s)
-            _lib.call("blade_beamform_detect_tc", buf.data_ptr(), plan.data_ptr(), out.data_ptr(), B, A, F, T, P, R,
-                      I, s)
+            _lib.call("blade_beamform_prepare_detect_tc", ph.data_ptr(), plan.data_ptr(), buf.data_ptr(),
+                      out.data_ptr(), B, A, F, T, P, R, I, s)
         else:
             _lib.call("blade_beamform_detect_f32", type_code(buf.dtype), buf.data_ptr(), ph.data_ptr(),
                       out.data_ptr(), B, A, F, T, P, R, I, s)

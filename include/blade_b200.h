@@ -234,6 +234,16 @@ BLADE_API int blade_beamform_detect_tc(const void* in, const void* plan, void* o
                              uint64_t B, uint64_t A, uint64_t F, uint64_t T,
                              uint64_t P, uint64_t rate, uint64_t integration,
                              blade_stream_t stream);
+/* blade_beamform_prepare_detect_tc: blade_beamform_tc_prepare followed by
+ * blade_beamform_detect_tc on the same stream, with the chain launched as a
+ * programmatic dependent of the split: its set-up and voltage loads overlap the
+ * split, and it reads the plan only after the split has finished.  Same
+ * arguments, limits and output as the two calls; `in` must be ready before
+ * the call is enqueued (stream order), as for blade_beamform_detect_tc. */
+BLADE_API int blade_beamform_prepare_detect_tc(const void* phasors, void* plan,
+                             const void* in, void* out, uint64_t B, uint64_t A,
+                             uint64_t F, uint64_t T, uint64_t P, uint64_t rate,
+                             uint64_t integration, blade_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * ATA ModeB in the reference's own order (pre-beamformer channelizer, per fine

@@ -133,6 +133,16 @@ def test_modeb_tensor_core_entry_points_validate_on_the_host():
         assert st == _lib.ERROR and word in msg, (word, msg)
 
 
+def test_prepare_detect_tc_validates_on_the_host():
+    # shape and buffer checks return before the split or the chain is enqueued
+    st, msg = _err("blade_beamform_prepare_detect_tc", None, None, None, None, 16, 28, 4, 100, 2, 4, 4, None)
+    assert st == _lib.ERROR and "unsupported" in msg  # T % 128
+    st, msg = _err("blade_beamform_prepare_detect_tc", None, None, None, None, 16, 65, 4, 128, 2, 4, 4, None)
+    assert st == _lib.ERROR and "unsupported" in msg  # A > 64
+    st, msg = _err("blade_beamform_prepare_detect_tc", None, None, None, None, 16, 28, 4, 128, 2, 4, 4, None)
+    assert st == _lib.ERROR and "null" in msg
+
+
 def test_meerkat_validation():
     st, msg = _err("blade_beamform_meerkat_f32", None, None, None, 2, 4, 3, 16, 3, 0, None)
     assert st == _lib.ERROR and "P must be" in msg

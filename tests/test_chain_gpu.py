@@ -69,6 +69,50 @@ def test_tensor_core_chain(cuda, name, A, F, T, B, R, I):
     np.testing.assert_array_equal(host(od2), y)
 
 
+@pytest.mark.parametrize("name,A,F,T,B,R,I", [CHAINS[1], CHAINS[4], CHAINS[5]])
+def test_prepare_detect_tc_matches_two_calls(cuda, name, A, F, T, B, R, I):
+    # the chain launched as a programmatic dependent of the split must read the
+    # split's new image, never the plan's previous contents: each call below
+    # rewrites the plan with different phasors
+    x, w1 = make(A, F, T, B, 4)
+    _, w2 = make(A, F, T, B, 5)
+    lib = _lib.load()
+    xd, w1d, w2d = dev(x), c64(w1), c64(w2)
+    plan = torch.full((int(lib.blade_beamform_tc_plan_size(B, A, F, 2)),), 0x7F, dtype=torch.uint8, device="cuda")
+    shape = (B, F * R, T // (R * I), 1)
+    expect = []
+    for wd in (w1d, w2d):
+        o = torch.zeros(shape, dtype=torch.float32, device="cuda")
+        call("blade_beamform_tc_prepare", ptr(wd), ptr(plan), B, A, F, 2, stream())
+        call("blade_beamform_detect_tc", ptr(xd), ptr(plan), ptr(o), B, A, F, T, 2, R, I, stream())
+        expect.append(host(o))
+    plan.fill_(0x7F)
+    for _ in range(3):
+        for wd, e in zip((w1d, w2d), expect):
+            o = torch.full(shape, float("nan"), dtype=torch.float32, device="cuda")
+            call("blade_beamform_prepare_detect_tc", ptr(wd), ptr(plan), ptr(xd), ptr(o), B, A, F, T, 2, R, I,
+                 stream())
+            np.testing.assert_array_equal(host(o), e)
+    assert bl.device_status() == 0
+    # captured into a CUDA graph (the programmatic edge is recorded), replayed alternately
+    side = torch.cuda.Stream()
+    outs = [torch.zeros(shape, dtype=torch.float32, device="cuda") for _ in range(2)]
+    graphs = []
+    with torch.cuda.stream(side):
+        for wd, o in zip((w1d, w2d), outs):
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=side):
+                call("blade_beamform_prepare_detect_tc", ptr(wd), ptr(plan), ptr(xd), ptr(o), B, A, F, T, 2, R, I,
+                     side.cuda_stream)
+            graphs.append(g)
+    for _ in range(3):
+        for g, o, e in zip(graphs, outs, expect):
+            o.fill_(float("nan"))
+            g.replay()
+            np.testing.assert_array_equal(host(o), e)
+    assert bl.device_status() == 0
+
+
 def test_tensor_core_matches_fp32_path(cuda):
     A, F, T, B, R, I = 28, 8, 2048, 16, 4, 4
     x, w = make(A, F, T, B, 3)
