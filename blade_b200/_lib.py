@@ -60,6 +60,7 @@ _SIGNATURES = {
     "blade_beamform_detect_tc_supported": (_int, [_u64, _u64, _u64, _u64, _u64, _u64, _u64]),
     "blade_beamform_detect_tc": (_int, [_vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),
     "blade_beamform_prepare_detect_tc": (_int, [_vp, _vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),
+    "blade_beamform_prepare_detect_tc_cf16": (_int, [_vp, _vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),
     "blade_beamform_detect_tc_cf16": (_int, [_vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),
     "blade_prechannelize_cf16": (_int, [_vp, _vp, _u64, _u64, _u64, _u64, _u64, _int, _vp]),
     "blade_incoherent_detect_cf16": (_int, [_vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp]),

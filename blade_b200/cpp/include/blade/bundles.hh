@@ -100,8 +100,8 @@ class Spectrometer : public Module {
 
 // ModeB's pre-beamformer stages and beamformer + detector on tensor cores for CI8
 // voltages at rate 2 or 4 (Stokes-I): blade_prechannelize_cf16 into an exact CF16
-// buffer, then the per-fine-channel phasor split and
-// blade_beamform_detect_tc_cf16, and with the incoherent beam its detected row
+// buffer, then the per-fine-channel phasor split and the chain
+// (blade_beamform_prepare_detect_tc_cf16), and with the incoherent beam its detected row
 // (blade_incoherent_detect_cf16).
 class ModeBTensorCore : public Module {
    public:
@@ -142,10 +142,10 @@ class ModeBTensorCore : public Module {
         const U64 B = input.phasors.shape()[0], R = config.rate;
         int rc = blade_prechannelize_cf16(input.buf.data(), pre.get().data(), s[0], s[1], s[2], 2, R,
                                           config.convertToCircular ? 1 : 0, stream);
-        if (!rc) rc = blade_beamform_tc_prepare(input.phasors.data(), plan.get().data(), B, s[0], s[1] * R, 2, stream);
         if (!rc)
-            rc = blade_beamform_detect_tc_cf16(pre.get().data(), plan.get().data(), out.get().data(), B, s[0],
-                                               s[1] * R, s[2] / R, 2, config.integrationSize, stream);
+            rc = blade_beamform_prepare_detect_tc_cf16(input.phasors.data(), plan.get().data(), pre.get().data(),
+                                                       out.get().data(), B, s[0], s[1] * R, s[2] / R, 2,
+                                                       config.integrationSize, stream);
         if (!rc && config.incoherentBeam)  // beam row B
             rc = blade_incoherent_detect_cf16(pre.get().data(), input.phasors.data(),
                                               out.get().data() + B * s[1] * R * (s[2] / (R * config.integrationSize)),

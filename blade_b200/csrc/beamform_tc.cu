@@ -1290,6 +1290,25 @@ extern "C" int blade_beamform_detect_tc_cf16(const void* in, const void* plan, v
                   pick_cf16(integration), stream);
 }
 
+extern "C" int blade_beamform_prepare_detect_tc_cf16(const void* phasors, void* plan, const void* in, void* out,
+                                                     uint64_t B, uint64_t A, uint64_t F, uint64_t T, uint64_t P,
+                                                     uint64_t integration, blade_stream_t stream) {
+    if (!blade_beamform_detect_tc_supported(B, A, F, T, P, 1, integration))
+        return set_error(BLADE_ERROR,
+                         "blade_beamform_prepare_detect_tc_cf16: unsupported configuration (B=%llu A=%llu T=%llu "
+                         "P=%llu I=%llu): needs P=2, 1<=A<=64, T%%128==0, I a power of two <= 32",
+                         (unsigned long long)B, (unsigned long long)A, (unsigned long long)T, (unsigned long long)P,
+                         (unsigned long long)integration);
+    if (!in || !plan || !out || !phasors)
+        return set_error(BLADE_ERROR, "blade_beamform_prepare_detect_tc_cf16: null buffer");
+    if (!aligned16(in) || !aligned16(plan) || (reinterpret_cast<uintptr_t>(out) & 3))
+        return set_error(BLADE_ERROR, "blade_beamform_prepare_detect_tc_cf16: input and plan must be 16-byte aligned");
+    if (F == 0) return BLADE_SUCCESS;
+    if (int rc = blade_beamform_tc_prepare(phasors, plan, B, A, F, P, stream)) return rc;
+    return tc_run("blade_beamform_prepare_detect_tc_cf16", in, plan, out, B, A, F, T, 1, integration, 8,
+                  pick_cf16(integration), stream, true);
+}
+
 extern "C" int blade_device_status(uint32_t* status) {
     unsigned int v = 0, zero = 0;
     cudaError_t e = cudaMemcpyFromSymbol(&v, g_tc_status, sizeof(v));
@@ -1354,6 +1373,5 @@ extern "C" int blade_beamform_detect_tc_noalloc(const void* in, const void* phas
                          (unsigned long long)need, (unsigned long long)kNoAllocPlanBytes);
     void* plan = nullptr;
     if (int rc = noalloc_plan_address(&plan)) return rc;
-    if (int rc = blade_beamform_tc_prepare(phasors, plan, B, A, F, P, stream)) return rc;
-    return blade_beamform_detect_tc(in, plan, out, B, A, F, T, P, rate, integration, stream);
+    return blade_beamform_prepare_detect_tc(phasors, plan, in, out, B, A, F, T, P, rate, integration, stream);
 }

@@ -805,8 +805,8 @@ class _ModeBTensorCore(Module):
     """ModeB on CI8 voltages with the detector (Stokes-I) at channelizer rate 2 or 4:
     the pre-beamformer Cast -> Channelizer -> [Polarizer] into an exact CF16 buffer
     (blade_prechannelize_cf16), then the per-fine-channel phasor split and the
-    tensor-core Beamformer -> Detector at rate 1 (blade_beamform_tc_prepare +
-    blade_beamform_detect_tc_cf16), and with the incoherent beam its detected row
+    tensor-core Beamformer -> Detector at rate 1 (blade_beamform_prepare_detect_tc_cf16:
+    the split, then the chain overlapping its end), and with the incoherent beam its detected row
     (blade_incoherent_detect_cf16).  Three or four launches."""
 
     taint = Taint.CONSUMER | Taint.PRODUCER
@@ -838,9 +838,8 @@ class _ModeBTensorCore(Module):
         A, F, T, P = x.shape
         B, R, sh = ph.shape[0], self._R, _stream_handle(stream)
         _lib.call("blade_prechannelize_cf16", x.data_ptr(), pre.data_ptr(), A, F, T, P, R, int(self._circ), sh)
-        _lib.call("blade_beamform_tc_prepare", ph.data_ptr(), plan.data_ptr(), B, A, F * R, P, sh)
-        _lib.call("blade_beamform_detect_tc_cf16", pre.data_ptr(), plan.data_ptr(), out.data_ptr(), B, A, F * R,
-                  T // R, P, self._I, sh)
+        _lib.call("blade_beamform_prepare_detect_tc_cf16", ph.data_ptr(), plan.data_ptr(), pre.data_ptr(),
+                  out.data_ptr(), B, A, F * R, T // R, P, self._I, sh)
         if self._inc:  # beam row B: the incoherent beam through the detector
             row = out.data_ptr() + B * F * R * (T // (R * self._I)) * 4
             _lib.call("blade_incoherent_detect_cf16", pre.data_ptr(), ph.data_ptr(), row, A, F * R, T // R, P,

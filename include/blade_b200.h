@@ -269,6 +269,14 @@ BLADE_API int blade_prechannelize_cf16(const void* in, void* out, uint64_t A, ui
 BLADE_API int blade_beamform_detect_tc_cf16(const void* in, const void* plan, void* out,
                                   uint64_t B, uint64_t A, uint64_t F, uint64_t T,
                                   uint64_t P, uint64_t integration, blade_stream_t stream);
+/* blade_beamform_prepare_detect_tc_cf16: blade_beamform_tc_prepare followed by
+ * blade_beamform_detect_tc_cf16, the chain launched as a programmatic dependent
+ * of the split (as blade_beamform_prepare_detect_tc does for CI8).  `in` must be
+ * ready before the call is enqueued. */
+BLADE_API int blade_beamform_prepare_detect_tc_cf16(const void* phasors, void* plan,
+                             const void* in, void* out, uint64_t B, uint64_t A,
+                             uint64_t F, uint64_t T, uint64_t P, uint64_t integration,
+                             blade_stream_t stream);
 
 /* Incoherent beam of Beamformer::ATA (src/modules/beamformer/beamformer.cu:64-78,
  * square-rooted because the detector follows, mode_b.hh:146-147) through the

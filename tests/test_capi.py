@@ -141,6 +141,10 @@ def test_prepare_detect_tc_validates_on_the_host():
     assert st == _lib.ERROR and "unsupported" in msg  # A > 64
     st, msg = _err("blade_beamform_prepare_detect_tc", None, None, None, None, 16, 28, 4, 128, 2, 4, 4, None)
     assert st == _lib.ERROR and "null" in msg
+    st, msg = _err("blade_beamform_prepare_detect_tc_cf16", None, None, None, None, 16, 28, 4, 100, 2, 4, None)
+    assert st == _lib.ERROR and "unsupported" in msg
+    st, msg = _err("blade_beamform_prepare_detect_tc_cf16", None, None, None, None, 16, 28, 4, 128, 2, 4, None)
+    assert st == _lib.ERROR and "null" in msg
 
 
 def test_meerkat_validation():

@@ -73,6 +73,14 @@ def test_tensor_core_fine_channels_match_oracle(cuda, A, F, T, B, R, I, circ):
     call("blade_beamform_detect_tc_cf16", ptr(y), ptr(plan), ptr(out), B, A, F * R, T // R, 2, I, stream())
     ref = O.mode_b(xh, wh, R, bool(circ), False, True, I, 1)
     assert rel_l2(host(out), ref) < TOL
+    # the split and the chain in one call (chain launched as the split's programmatic
+    # dependent): the same bits, from a plan that first holds other phasors
+    w2 = dev(phasors(B, A, F * R, I + 100))
+    call("blade_beamform_tc_prepare", ptr(w2), ptr(plan), B, A, F * R, 2, stream())
+    out2 = torch.full_like(out, float("nan"))
+    call("blade_beamform_prepare_detect_tc_cf16", ptr(w), ptr(plan), ptr(y), ptr(out2), B, A, F * R, T // R, 2, I,
+         stream())
+    np.testing.assert_array_equal(host(out2), host(out))
 
 
 def test_modeb_module_takes_the_tensor_core_path(cuda):
