@@ -26,6 +26,10 @@ CHAINS = [
     ("ragged-beams", 13, 3, 512, 37, 4, 2),
     ("many-beams", 9, 2, 256, 100, 1, 1),
     ("window32", 16, 2, 1024, 16, 1, 32),
+    # rate 4: few antennas (padded K), a full 32-antenna K, windows of 1, 8 and 32
+    ("tmem-operand-5ant", 5, 3, 256, 3, 4, 1),
+    ("tmem-operand-32ant", 32, 2, 1024, 16, 4, 32),
+    ("tmem-operand-i8", 17, 5, 2048, 9, 4, 8),
 ]
 
 
