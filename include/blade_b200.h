@@ -299,8 +299,8 @@ BLADE_API int blade_device_status(uint32_t* status);
 
 /* ---------------------------------------------------------------------------
  * Allocation-free tensor-core chain (no counterpart in the reference).
- * Same computation, arguments and output as blade_beamform_tc_prepare followed
- * by blade_beamform_detect_tc, but the phasor image lives in a fixed 8 MiB
+ * Same computation, arguments and output as blade_beamform_prepare_detect_tc
+ * (the split, then the chain overlapping its end), but the phasor image lives in a fixed 8 MiB
  * device array inside this library instead of caller-allocated memory, so the
  * call itself allocates nothing (no cudaMalloc / cudaFree).  It is meant for
  * streaming callers whose device memory is sized once at start-up and whose
