@@ -231,7 +231,7 @@ def duplicate(x: np.ndarray) -> np.ndarray:
 
 
 # --------------------------------------------------------------------------- #
-# Chains (bundles and the BASELINE workloads)
+# Chains (bundles and the benchmark workloads)
 # --------------------------------------------------------------------------- #
 
 def beamform_channelize_detect(x_ci8: np.ndarray, phasors: np.ndarray, rate: int,
