@@ -34,6 +34,39 @@ def test_library_exports_every_declared_symbol():
         assert s in _lib.exported_symbols(), f"{s} has no ctypes signature"
 
 
+def _header_prototypes():
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for ret, name, params in re.findall(r"BLADE_API\s+([\w\s\*]+?)\b(blade_\w+)\s*\(([^)]*)\)\s*;", text, flags=re.S):
+        ps = [" ".join(p.split()) for p in params.split(",")]
+        out[name] = (" ".join(ret.split()), [p for p in ps if p and p != "void"])
+    return out
+
+
+def _ctype_ok(decl, ct):
+    """Whether ctypes type `ct` passes a C parameter (or return) declared as `decl`."""
+    if "*" in decl or "[" in decl:
+        if decl.startswith("const char"):
+            return ct in (ctypes.c_char_p, ctypes.c_void_p)
+        return ct is ctypes.c_void_p or (isinstance(ct, type) and issubclass(ct, ctypes._Pointer))
+    base = re.sub(r"\s+\w+$", "", decl) if " " in decl else decl
+    return {"uint64_t": ctypes.c_uint64, "int": ctypes.c_int, "double": ctypes.c_double,
+            "blade_stream_t": ctypes.c_void_p, "uint32_t": ctypes.c_uint32}.get(base) is ct
+
+
+def test_ctypes_signatures_match_the_header():
+    # argument count, integer widths and pointer-versus-value for every entry point,
+    # so a reordered or widened C parameter cannot drift silently from the binding
+    protos = _header_prototypes()
+    assert set(protos) == set(declared_symbols())
+    for name, (ret, params) in protos.items():
+        res, args = _lib._SIGNATURES[name]
+        assert len(args) == len(params), (name, len(args), len(params))
+        assert _ctype_ok(ret + (" r" if "*" not in ret else ""), res), (name, ret, res)
+        for i, (decl, ct) in enumerate(zip(params, args)):
+            assert _ctype_ok(decl, ct), (name, i, decl, ct)
+
+
 def test_version():
     assert _lib.load().blade_version() == 10000
 
