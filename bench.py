@@ -2,53 +2,67 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload (ATA production chain, seeded synthetic data): A = 28 antennas,
-F = 192 channels, T = 8192 samples, P = 2 polarisations, B = 16 beams, CI8
-voltages (sigma 8, clipped to +-127), phasors exp(-i 2 pi f tau) with
-f = 6.0 GHz + 0.5 MHz k, tau ~ U[-5 us, 5 us]; Cast -> Beamformer ->
-Channelizer (rate 4) -> Detector (Stokes-I, integration 4).
+Headline workload (the dense beamformer block, seeded synthetic data): A = 64
+antennas, B = 64 beams, F = 256 channels, T = 8192 samples, P = 2
+polarisations, CI8 voltages (sigma 8, clipped to +-127), phasors
+exp(-i 2 pi f tau) with f = 6.0 GHz + 0.5 MHz k, tau ~ U[-5 us, 5 us];
+Cast -> Beamformer -> Detector (Stokes-I, integration 8).
 
 One step = one pass of the chain over one block: phasor hi/lo split + the fused
 tcgen05 kernel.  value = 4 B A F T P / t in TMAC/s (whole job); the JSON line
 also carries the ingest rate, the plain FP32 CUDA-core path on the same block,
-the dense 64 x 64 workload (A = B = 64, F = 256, T = 8192, I = 8) for both
-paths, the roofline of the dominant kernel, the CPU baseline (the reference's
-numpy formulas, FP64, on a bounded channel sample) and the end-to-end rate
-through the public Runner API with host buffers.  Three further legs cover the
-other measured workloads: the high-resolution spectrometer (A = 1, F = 64,
-T = 2^20, Cast -> Channelizer(65536) -> Polarizer -> Detector I = 8), the small
-block's launch latency eager against one CUDA graph (A = 20, F = 96, T = 256,
-B = 8; also as one fused FP32 launch and as the tensor-core pair), the forward +
-adjoint step of the Stokes loss (A = 28, B = 1, F = 192, T = 2048, CF32) and the
-ATA ModeB bundle in the reference's order on the production block
-(pre-beamformer channelizer, per-fine-channel phasors; the tensor-core path with
-and without the incoherent beam, and the module chain);
---skip-extra leaves them out.
+the roofline of the dominant kernel (tensor-bound: the FP16-split contraction's
+tensor FLOPs against the measured bf16 peak), the CPU baseline (the reference's
+numpy formulas, FP64, on a bounded channel sample, which also checks the GPU
+Stokes-I of those channels against FP64) and the end-to-end rate through the
+public Runner API with host buffers (voltages and delays in, Stokes-I out).
 
-Multi-GPU (torchrun): weak scaling, every rank owns its own 192-channel band
+Further legs: the ATA production chain (A = 28, F = 192, T = 8192, B = 16,
+Channelizer rate 4, I = 4) on both paths with its HBM roofline; the
+high-resolution spectrometer (A = 1, F = 64, T = 2^20, Cast ->
+Channelizer(65536) -> Polarizer -> Detector I = 8); the small block's launch
+latency eager against one CUDA graph (A = 20, F = 96, T = 256, B = 8); the
+forward + adjoint step of the Stokes loss (A = 28, B = 1, F = 192, T = 2048,
+CF32); the ATA ModeB bundle in the reference's order; the byte-movement modules
+(Gather, Permutation, Duplicate) and the standalone Channelizer on the
+reference's own benchmark shapes; --skip-extra leaves them out.
+
+Multi-GPU (torchrun): weak scaling, every rank owns its own 256-channel band
 (frequency sharding, no data-path collective); time = max over ranks.
 """
 
 from __future__ import annotations
 
-import argparse
-import json
 import os
-import statistics
-import subprocess
-import sys
-import threading
-import time
 
-import numpy as np
-import torch
+# The CPU legs (numpy + BLAS) use every host core the process may run on; the
+# thread counts are set before numpy loads its BLAS and reported with the numbers.
+CORES = len(os.sched_getaffinity(0))
+THREAD_VARS = ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")
+for _v in THREAD_VARS:
+    os.environ.setdefault(_v, str(CORES))
+
+import argparse  # noqa: E402
+import json  # noqa: E402
+import statistics  # noqa: E402
+import subprocess  # noqa: E402
+import sys  # noqa: E402
+import threading  # noqa: E402
+import time  # noqa: E402
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORK = dict(A=28, F=192, T=8192, P=2, B=16, R=4, I=4)
 DENSE = dict(A=64, F=256, T=8192, P=2, B=64, R=1, I=8)
+ATA = dict(A=28, F=192, T=8192, P=2, B=16, R=4, I=4)
+SEED = {"dense": 1003, "ata": 1002}
+HEAD = DENSE
 METRIC = "Beamform+detect TMAC/s & ingest GB/s: FP16-split TC vs FP32 at <=1e-5 rel err"
+WORKLOAD_NAME = ("dense beamformer block: A=64 B=64 F=256 T=8192 P=2 CI8, Cast->Beamformer->Detector"
+                 "(Stokes-I, I=8)")
 
 
 def tmac(w):
@@ -65,6 +79,22 @@ def algorithmic_bytes(w):
     return ingest_bytes(w) + w["B"] * w["A"] * w["F"] * w["P"] * 8 + out
 
 
+def split_tensor_flops(w):
+    # FP16-split contraction: the hi and the lo phasor products, 2 flop per real MAC.
+    return 2.0 * 2.0 * tmac(w)
+
+
+def bench_config(world):
+    """The config dict both arms print (identical for the same world size)."""
+    return {"workload": WORKLOAD_NAME,
+            "l2": "inputs larger than L2 (537 MB CI8 per block vs 126 MB L2)",
+            "parallelism": f"frequency-sharded x{world} (weak)"}
+
+
+def thread_settings():
+    return {"cores": CORES, **{v: os.environ.get(v) for v in THREAD_VARS}}
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -75,9 +105,9 @@ def load_peaks():
         return 6650.0, 1590.0, "fallback"
 
 
-def load_traffic():
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "bf_tc_kernel_ata_production.md")
+def load_traffic(name):
+    """Per-launch DRAM bytes of a kernel from its committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(p):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -167,13 +197,12 @@ def max_over_ranks(x: float, world: int) -> float:
 
 
 # --------------------------------------------------------------------------- data
-def make_inputs(w, seed, device=True):
+def make_inputs(w, seed):
+    """Host CI8 voltages [A, F, T, P, 2] and delays [B, A] (seconds, FP64)."""
     g = torch.Generator().manual_seed(seed)
     x = torch.randn((w["A"], w["F"], w["T"], w["P"], 2), generator=g, dtype=torch.float32) * 8.0
     x = x.round_().clamp_(-127, 127).to(torch.int8)
     tau = (torch.rand((w["B"], w["A"]), generator=g, dtype=torch.float64) * 2 - 1) * 5e-6
-    if device:
-        return x.cuda(), tau.cuda()
     return x, tau
 
 
@@ -207,12 +236,10 @@ def time_path(w, x, ph, path, steps, warmup, world):
                       out.data_ptr(), B, A, F, T, P, R, I, sh)
         elif path == "tc":  # the same two kernels as separate calls, events around the chain
             _lib.call("blade_beamform_tc_prepare", ph.data_ptr(), plan.data_ptr(), B, A, F, P, sh)
-            if ev is not None:
-                ev[0].record(s)
+            ev[0].record(s)
             _lib.call("blade_beamform_detect_tc", x.data_ptr(), plan.data_ptr(), out.data_ptr(), B, A, F, T, P, R, I,
                       sh)
-            if ev is not None:
-                ev[1].record(s)
+            ev[1].record(s)
         else:
             if ev is not None:
                 ev[0].record(s)
@@ -252,11 +279,15 @@ def time_path(w, x, ph, path, steps, warmup, world):
     return max_over_ranks(total / steps, world), kern, out, launches
 
 
-def e2e_runner(w, steps, warmup, world):
-    """End to end through the public Runner API: per step H2D of the block's CI8
-    voltages and phasors from pinned host memory, the fused chain, D2H of the
-    Stokes-I result; the two Runner slots overlap copies and compute."""
+def e2e_runner(w, x, tau, steps, warmup, world):
+    """End to end through the public Runner API, as a streaming caller uses it:
+    per step the H2D copy of the block's CI8 voltages and of the per-block delays
+    [B, A] from pinned host memory, the Phasor module (delays -> phasors on the
+    device, FP64) and the fused chain, then the D2H copy of the Stokes-I result;
+    the two Runner slots overlap copies and compute.  Returns (ms per step, H2D
+    bytes, D2H bytes, the last step's output on the host)."""
     import blade_b200 as bl
+    from blade_b200.synthetic import DF_HZ, F0_HZ
 
     B, A, F, T, P, R, I = (w[k] for k in ("B", "A", "F", "T", "P", "R", "I"))
 
@@ -264,22 +295,25 @@ def e2e_runner(w, steps, warmup, world):
     class Chain:
         def __init__(self):
             self.input.buf = bl.array_tensor((A, F, T, P), dtype=bl.ci8)
-            self.input.phasors = bl.phasor_tensor((B, A, F, 1, P), dtype=bl.cf32)
+            self.input.delays = bl.delay_tensor((B, A), dtype=bl.f64)
             self.output.buf = bl.array_tensor((B, F * R, T // (R * I), 1), dtype=bl.f32)
+            self.module.phasor = bl.module(bl.phasor, {"number_of_beams": B, "number_of_antennas": A,
+                                                       "number_of_frequency_channels": F,
+                                                       "number_of_polarizations": P,
+                                                       "observation_frequency_hz": F0_HZ,
+                                                       "channel_bandwidth_hz": DF_HZ, "total_bandwidth_hz": 0.0},
+                                           (self.input.delays,), telescope=bl.ata)
             self.module.bd = bl.module(bl.beamform_detect, {"rate": R, "integration_size": I},
-                                       (self.input.buf, self.input.phasors), telescope=bl.ata)
+                                       (self.input.buf, self.module.phasor.get_phasors()), telescope=bl.ata)
 
     p = Chain()
-    x, tau = make_inputs(w, 2002, device=False)
     hx = [bl.array_tensor((A, F, T, P), dtype=bl.ci8, device=bl.cpu) for _ in range(2)]
-    hw = [bl.phasor_tensor((B, A, F, 1, P), dtype=bl.cf32, device=bl.cpu) for _ in range(2)]
+    hd = [bl.delay_tensor((B, A), dtype=bl.f64, device=bl.cpu) for _ in range(2)]
     ho = [bl.array_tensor((B, F * R, T // (R * I), 1), dtype=bl.f32, device=bl.cpu) for _ in range(2)]
-    ph = phasors_on_device(tau.cuda(), w, torch.cuda.current_stream().cuda_stream)
     for k in range(2):
         hx[k].as_torch().copy_(x)
-        hw[k].as_torch().copy_(ph.cpu())
-    torch.cuda.synchronize()
-    h2d = hx[0].nbytes + hw[0].nbytes
+        hd[k].as_torch().copy_(tau)
+    h2d = hx[0].nbytes + hd[0].nbytes
     d2h = ho[0].nbytes
 
     def run(n):
@@ -290,7 +324,7 @@ def e2e_runner(w, steps, warmup, world):
 
                 def cin(j=j):
                     p.copy(p.input.buf, hx[j])
-                    p.copy(p.input.phasors, hw[j])
+                    p.copy(p.input.delays, hd[j])
 
                 def cout(j=j):
                     p.copy(p.output.buf, p.module.bd.get_output())
@@ -317,8 +351,9 @@ def e2e_runner(w, steps, warmup, world):
     torch.cuda.synchronize()
     ms = max(start.elapsed_time(e0), start.elapsed_time(e1)) / steps
     barrier(world)
+    last = ho[(steps - 1) % 2].as_torch().clone()
     p.runner.release_graphs()
-    return max_over_ranks(ms, world), h2d, d2h
+    return max_over_ranks(ms, world), h2d, d2h, last
 
 
 SPECTRO = dict(A=1, F=64, T=1 << 20, P=2, R=65536, I=8)
@@ -500,7 +535,7 @@ def modeb_step(steps, warmup):
     import blade_b200 as bl
     from blade_b200.modules import BeamformerATA, Cast, Channelizer, Detector
 
-    w = dict(WORK)
+    w = dict(ATA)
     A, F, T, P, B, R, I = (w[k] for k in ("A", "F", "T", "P", "B", "R", "I"))
     g = torch.Generator(device="cuda").manual_seed(1006)
     buf = bl.array_tensor((A, F, T, P), dtype=bl.ci8, device=bl.cuda)
@@ -588,34 +623,148 @@ def adjoint_step(steps, warmup):
             "macs_fwd_plus_adj": 2 * 4 * B * A * F * T * P}
 
 
-def cpu_baseline(w, out_gpu, budget_s=10.0):
-    """The reference's numpy formulas (FP64 oracle restatement) on a bounded
-    channel sample of the same block, on every host core; also checks the GPU
-    output of those channels against FP64."""
+GATHER_SHAPES = [("ata", (5, 192, 8192, 2)), ("vla", (5, 131072, 1, 2))]
+PERMUTATIONS = [("AFTP", (0, 1, 2, 3)), ("ATFP", (0, 2, 1, 3)), ("ATPF", (0, 2, 3, 1))]
+
+
+def copies(steps, warmup):
+    """Byte-movement modules on the reference's own benchmark shapes, CF32:
+    Gather axis 2, multiplier 64 of [5, 192, 8192, 2] (ATA) and [5, 131072, 1, 2]
+    (VLA) inputs (benchmarks/modules/gather/generic.hh:13-32); Permutation of
+    [2, 192, 8192, 2] as AFTP, ATFP, ATPF (benchmarks/modules/permutation/
+    generic.hh:11-17); Duplicate of [20, 192, 8192, 2]
+    (benchmarks/modules/duplicate/base.hh:19).  GB/s = bytes read + written per
+    call / device time per call (CUDA events around back-to-back calls)."""
+    from blade_b200 import _lib
+
+    _lib.load()
+    hbm = load_peaks()[0]
+    s = torch.cuda.current_stream()
+    sh = s.cuda_stream
+
+    def timed(fn, nbytes):
+        for _ in range(warmup):
+            fn(0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for k in range(steps):
+            fn(k)
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        return {"ms": round(ms, 4), "bytes": nbytes, "gbs": round(gbs, 1), "frac_of_hbm": round(gbs / hbm, 3)}
+
+    res = {"hbm_peak_gbs": hbm}
+    mult = 64
+    for name, shape in GATHER_SHAPES:
+        n = int(np.prod(shape))
+        x = torch.randn(n * 2, device="cuda").view(torch.complex64)
+        oshape = list(shape)
+        oshape[2] *= mult
+        y = torch.empty(n * mult, dtype=torch.complex64, device="cuda")
+        shp = _lib.u64_array(shape)
+        res[f"gather_{name}"] = timed(
+            lambda k: _lib.call("blade_gather", 8, x.data_ptr(), y.data_ptr(), shp, 2, mult, k % mult, sh), 16 * n)
+        del x, y
+    shape = (2, 192, 8192, 2)
+    n = int(np.prod(shape))
+    x = torch.randn(n * 2, device="cuda").view(torch.complex64)
+    y = torch.empty_like(x)
+    shp = _lib.u64_array(shape)
+    for name, idx in PERMUTATIONS:
+        ix = _lib.u64_array(idx)
+        res[f"permute_{name}"] = timed(lambda k: _lib.call("blade_permute", 8, x.data_ptr(), y.data_ptr(), shp, ix, sh),
+                                       16 * n)
+    del x, y
+    n = 20 * 192 * 8192 * 2
+    x = torch.randn(n * 2, device="cuda").view(torch.complex64)
+    y = torch.empty_like(x)
+    res["duplicate"] = timed(lambda k: _lib.call("blade_duplicate", x.data_ptr(), y.data_ptr(), 8 * n, sh), 16 * n)
+    del x, y
+    res["shapes"] = ("gather axis 2 x64 of CF32 [5,192,8192,2] and [5,131072,1,2]; permute CF32 [2,192,8192,2]; "
+                     "duplicate CF32 [20,192,8192,2]")
+    return res
+
+
+def channelizer_module(steps, warmup):
+    """The standalone Channelizer module, CF32 in and out, one launch per call:
+    rate 4 on the ATA beams [16, 192, 8192, 2] (the ATA production chain's
+    channelizer as a separate module) and rate 8192 on [16, 192, 8192, 2]
+    (benchmarks/modules/channelizer/generic.hh:13-17).  GB/s counts the kernel's
+    own reads and writes (input, output, and a workspace round trip where the
+    four-step path uses one)."""
+    from blade_b200 import _lib
+
+    lib = _lib.load()
+    hbm = load_peaks()[0]
+    s = torch.cuda.current_stream()
+    sh = s.cuda_stream
+    A, F, T, P = 16, 192, 8192, 2
+    n = A * F * T * P
+    x = torch.randn(n * 2, device="cuda").view(torch.complex64)
+    res = {"hbm_peak_gbs": hbm}
+    for R in (4, 8192):
+        y = torch.empty_like(x)
+        wsb = int(lib.blade_channelize_workspace_size(A, F, T, P, R))
+        ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
+
+        def fn():
+            _lib.call("blade_channelize", x.data_ptr(), y.data_ptr(), ws.data_ptr() if wsb else None, A, F, T, P, R, sh)
+
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(steps):
+            fn()
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        nbytes = (32 if wsb else 16) * n
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        res[f"rate{R}"] = {"ms": round(ms, 4), "bytes": nbytes, "gbs": round(gbs, 1), "frac_of_hbm": round(gbs / hbm, 3),
+                           "workspace": bool(wsb)}
+        del y, ws
+    res["shape"] = "CF32 [16, 192, 8192, 2]"
+    del x
+    return res
+
+
+def cpu_reference_sample(w, x, tau, budget_s):
+    """The reference's numpy formulas (FP64 restatement of its test oracles) on the
+    first nch channels of the block, nch sized so the run takes about budget_s.
+    Returns (Stokes-I of those channels, nch, seconds)."""
+    from blade_b200.synthetic import phasors_from_delays
     from oracle import formulas as O
 
-    x, tau = make_inputs(w, 1002, device=False)
-    x = x.numpy()
-    from blade_b200.synthetic import phasors_from_delays
-
+    xn = x.numpy()
     ph = phasors_from_delays(tau.numpy(), w["F"], w["P"])
-    cores = len(os.sched_getaffinity(0))
-    # one channel to size the sample
     t = time.perf_counter()
-    O.beamform_channelize_detect(x[:, :1], ph[:, :, :1], w["R"], w["I"])
+    O.beamform_channelize_detect(xn[:, :1], ph[:, :, :1], w["R"], w["I"])
     one = max(time.perf_counter() - t, 1e-3)
     nch = int(max(1, min(w["F"], budget_s / one)))
     t = time.perf_counter()
-    ref = O.beamform_channelize_detect(x[:, :nch], ph[:, :, :nch], w["R"], w["I"])
-    dt = time.perf_counter() - t
+    ref = O.beamform_channelize_detect(xn[:, :nch], ph[:, :, :nch], w["R"], w["I"])
+    return ref, nch, time.perf_counter() - t
+
+
+def cpu_baseline(w, x, tau, outs, budget_s=10.0):
+    """CPU baseline on the host cores plus the FP64 check of the GPU Stokes-I
+    (each output in `outs`) on the same channel sample."""
+    ref, nch, dt = cpu_reference_sample(w, x, tau, budget_s)
+    errs = {}
+    for name, out in outs.items():
+        got = out[:, : nch * w["R"]].cpu().numpy()
+        errs[name] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
     sample = dict(w, F=nch)
-    err = None
-    if out_gpu is not None:
-        got = out_gpu[:, : nch * w["R"]].cpu().numpy()
-        err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
-    return {"value": tmac(sample) / dt / 1e12, "unit": "TMAC/s", "cores": cores, "kind": "port",
-            "sample": f"{nch} of {w['F']} channels of the block (FP64 numpy: matmul beamform, np.fft channelize, "
-                      f"reshape-sum detect), {dt:.1f} s"}, err
+    base = {"value": tmac(sample) / dt / 1e12, "unit": "TMAC/s", "cores": CORES, "kind": "port",
+            "threads": thread_settings(),
+            "sample": f"{nch} of {w['F']} channels of the block, a per-channel rate (FP64 numpy: matmul beamform, "
+                      f"np.fft channelize, reshape-sum detect), {dt:.1f} s"}
+    return base, errs, nch
 
 
 # --------------------------------------------------------------------------- arms
@@ -625,22 +774,31 @@ def run_ours(args):
 
     _lib.load()
     hbm_peak, tc_peak, peak_kind = load_peaks()
-    w = WORK
+    w = HEAD
     stream = torch.cuda.current_stream().cuda_stream
-    x, tau = make_inputs(w, 1002 + rank)
+    hx, htau = make_inputs(w, SEED["dense"] + rank)
+    x, tau = hx.cuda(), htau.cuda()
     ph = phasors_on_device(tau, w, stream)
     with ClockSampler(local) as clk:
         ms_tc, kern_tc, out_tc, launches = time_path(w, x, ph, "tc", args.steps, args.warmup, world)
         ms_tc_separate = time_path.separate_ms
-        ms_f32, kern_f32, out_f32, _ = time_path(w, x, ph, "f32", args.steps, args.warmup, world)
-        e2e_ms, h2d, d2h = e2e_runner(w, max(4, min(args.steps, 20)), args.warmup, world)
-        # dense 64 x 64 workload, both paths
-        xd, taud = make_inputs(DENSE, 1003 + rank)
-        phd = phasors_on_device(taud, DENSE, stream)
-        dms_tc, dk_tc, dout_tc, _ = time_path(DENSE, xd, phd, "tc", max(3, args.steps // 4), args.warmup, world)
-        dms_f32, dk_f32, dout_f32, _ = time_path(DENSE, xd, phd, "f32", max(3, args.steps // 8), args.warmup, world)
-        dense_agree = float((dout_tc - dout_f32).norm() / dout_f32.norm())
-        del xd, phd, dout_tc, dout_f32
+        f32_steps = max(3, args.steps // 4)
+        ms_f32, kern_f32, out_f32, _ = time_path(w, x, ph, "f32", f32_steps, args.warmup, world)
+        tc_vs_f32 = float((out_tc - out_f32).norm() / out_f32.norm())
+        out_tc_h, out_f32_h = out_tc.cpu(), out_f32.cpu()
+        del x, ph, out_tc, out_f32
+        torch.cuda.synchronize()
+        e2e_ms, h2d, d2h, e2e_out = e2e_runner(w, hx, htau, max(4, min(args.steps, 16)), args.warmup, world)
+        e2e_vs_device = float((e2e_out - out_tc_h).norm() / out_tc_h.norm())
+        # the ATA production chain (A=28 F=192 T=8192 B=16, rate 4, I=4), both paths
+        ax, atau = make_inputs(ATA, SEED["ata"] + rank)
+        ax = ax.cuda()
+        aph = phasors_on_device(atau.cuda(), ATA, stream)
+        ams_tc, akern_tc, aout_tc, _ = time_path(ATA, ax, aph, "tc", args.steps, args.warmup, world)
+        ams_tc_separate = time_path.separate_ms
+        ams_f32, _, aout_f32, _ = time_path(ATA, ax, aph, "f32", max(3, args.steps // 2), args.warmup, world)
+        ata_agree = float((aout_tc - aout_f32).norm() / aout_f32.norm())
+        del ax, aph, aout_tc, aout_f32
         torch.cuda.synchronize()
         extra = {}
         if not args.skip_extra and world == 1:
@@ -648,6 +806,8 @@ def run_ours(args):
             extra["small_block_latency"] = small_block_latency(100)
             extra["adjoint"] = adjoint_step(max(5, args.steps // 2), args.warmup)
             extra["modeb"] = modeb_step(max(3, args.steps // 6), args.warmup)
+            extra["copies"] = copies(max(5, args.steps // 2), args.warmup)
+            extra["channelizer_module"] = channelizer_module(max(5, args.steps // 4), args.warmup)
         torch.cuda.synchronize()
     clocks = clk.summary()
     if rank != 0:
@@ -657,9 +817,11 @@ def run_ours(args):
             dist.destroy_process_group()
         return
     value = world * tmac(w) / (ms_tc * 1e-3) / 1e12
-    achieved = algorithmic_bytes(w) / (kern_tc * 1e-3) / 1e9
-    traffic = load_traffic()
-    base, err = cpu_baseline(w, out_tc) if world == 1 else (None, None)
+    tflops = split_tensor_flops(w) / (kern_tc * 1e-3) / 1e12
+    base, errs, nch = (None, {}, 0)
+    if world == 1:
+        base, errs, nch = cpu_baseline(w, hx, htau, {"tc": out_tc_h, "f32": out_f32_h})
+    a_achieved = algorithmic_bytes(ATA) / (akern_tc * 1e-3) / 1e9
     line = {
         "metric": METRIC,
         "value": round(value, 4),
@@ -673,31 +835,46 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f16 hi+lo split, f32 accumulate",
         "data": "synthetic (seeded CI8 sigma 8, delays U[-5us,5us]); no dataset",
-        "config": {"workload": "ATA production chain: A=28 F=192 T=8192 P=2 B=16, Cast->Beamformer->"
-                               "Channelizer(rate 4)->Detector(Stokes-I, I=4)",
-                   "l2": "inputs larger than L2 (176 MB CI8 per block vs 126 MB L2)",
-                   "parallelism": f"frequency-sharded x{world} (weak)"},
+        "config": bench_config(world),
         "ingest_gbs": round(world * ingest_bytes(w) / (ms_tc * 1e-3) / 1e9, 2),
+        "stokes_rel_err_vs_fp64": errs.get("tc"),
         "fp32_path": {"tmacs": round(world * tmac(w) / (ms_f32 * 1e-3) / 1e12, 4), "ms_per_step": round(ms_f32, 6),
-                      "speedup_tc_over_fp32": round(ms_f32 / ms_tc, 3)},
-        "dense_64x64": {"workload": "A=64 B=64 F=256 T=8192 P=2 rate 1 I=8",
-                        "tc_tmacs": round(world * tmac(DENSE) / (dms_tc * 1e-3) / 1e12, 3),
-                        "fp32_tmacs": round(world * tmac(DENSE) / (dms_f32 * 1e-3) / 1e12, 3),
-                        "speedup_tc_over_fp32": round(dms_f32 / dms_tc, 3),
-                        "tc_kernel_ms": round(dk_tc, 4),
-                        "tensor_frac_of_measured_bf16": round(2 * tmac(DENSE) / (dk_tc * 1e-3) / 1e12 / tc_peak, 4),
-                        "tc_vs_fp32_rel_l2": dense_agree},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                     "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
-                     "kernel": "bf_tc_kernel<4>", "peak_kind": f"{peak_kind} hbm_gbs (burst)",
-                     "algorithmic_bytes_per_launch": algorithmic_bytes(w), "kernel_ms": round(kern_tc, 5),
-                     "step_ms_separate_calls": round(ms_tc_separate, 5)},
+                      "speedup_tc_over_fp32": round(ms_f32 / ms_tc, 3),
+                      "stokes_rel_err_vs_fp64": errs.get("f32"), "tc_vs_fp32_rel_l2": tc_vs_f32},
+        "fp64_check": f"first {nch} of {w['F']} channels (all beams, all samples) against the FP64 numpy chain",
+        "roofline": {"bound": "tensor", "achieved": round(tflops, 1), "peak": tc_peak, "unit": "TFLOP/s",
+                     "frac": round(tflops / tc_peak, 4), "traffic": load_traffic("bf_tc_kernel_dense_64x64.md"),
+                     "kernel": "bf_tc_kernel<1,3>", "peak_kind": f"{peak_kind} bf16_tflops (burst)",
+                     "flops_per_launch": split_tensor_flops(w),
+                     "flops_counted": "FP16-split contraction: hi and lo products, 2 flop per real MAC, "
+                                      "4 B A F T P real MACs each",
+                     "useful_frac": round(0.5 * tflops / tc_peak, 4),
+                     "kernel_ms": round(kern_tc, 5), "step_ms_separate_calls": round(ms_tc_separate, 5),
+                     "hbm_view": {"algorithmic_bytes_per_launch": algorithmic_bytes(w),
+                                  "gbs": round(algorithmic_bytes(w) / (kern_tc * 1e-3) / 1e9, 1),
+                                  "frac": round(algorithmic_bytes(w) / (kern_tc * 1e-3) / 1e9 / hbm_peak, 4)}},
         "cpu_baseline": base,
-        "stokes_rel_err_vs_fp64": err,
         "e2e": {"value": round(world * tmac(w) / (e2e_ms * 1e-3) / 1e12, 4), "unit": "TMAC/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 4),
-                "api": "bl.runner(graph=True) + bl.module(bl.beamform_detect) enqueue/dequeue"},
-        "gpu_launches": launches * args.steps,
+                "rel_l2_vs_device_path": e2e_vs_device,
+                "api": "bl.runner(graph=True): bl.module(bl.phasor) (delays in) + bl.module(bl.beamform_detect), "
+                       "enqueue/dequeue with pinned host buffers"},
+        "ata_production": {
+            "workload": "ATA production chain: A=28 F=192 T=8192 P=2 B=16, Cast->Beamformer->Channelizer(rate 4)"
+                        "->Detector(Stokes-I, I=4)",
+            "tc_tmacs": round(world * tmac(ATA) / (ams_tc * 1e-3) / 1e12, 4), "tc_ms_per_step": round(ams_tc, 5),
+            "fp32_tmacs": round(world * tmac(ATA) / (ams_f32 * 1e-3) / 1e12, 4),
+            "speedup_tc_over_fp32": round(ams_f32 / ams_tc, 3), "tc_vs_fp32_rel_l2": ata_agree,
+            "ingest_gbs": round(world * ingest_bytes(ATA) / (ams_tc * 1e-3) / 1e9, 2),
+            "roofline": {"bound": "hbm", "achieved": round(a_achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                         "frac": round(a_achieved / hbm_peak, 4),
+                         "traffic": load_traffic("bf_tc_kernel_ata_production.md"), "kernel": "bf_tc_kernel<4,2>",
+                         "peak_kind": f"{peak_kind} hbm_gbs (burst)",
+                         "algorithmic_bytes_per_launch": algorithmic_bytes(ATA), "kernel_ms": round(akern_tc, 5),
+                         "step_ms_separate_calls": round(ams_tc_separate, 5)}},
+        "gpu_launches": launches * args.steps * 2 + f32_steps * 2,
+        "gpu_launches_counted": "headline tc loop (split + chain per step) run twice (fused call, then separate "
+                                "calls with events), plus the fp32 loops; warm-up excluded",
         "clocks": clocks,
     }
     line.update(extra)
@@ -709,17 +886,19 @@ def run_ours(args):
 
 
 def run_reference(args):
+    """The reference's CPU formula for the path (its tests' numpy oracles, restated in
+    FP64) on the host cores, on the headline block, a bounded channel sample per step."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    w = WORK
-    from oracle import formulas as O
+    w = HEAD
     from blade_b200.synthetic import phasors_from_delays
+    from oracle import formulas as O
 
-    x, tau = make_inputs(w, 1002, device=False)
-    x = x.numpy()
-    ph = phasors_from_delays(tau.numpy(), w["F"], w["P"])
-    cores = len(os.sched_getaffinity(0))
+    hx, htau = make_inputs(w, SEED["dense"])
+    x = hx.numpy()
+    ph = phasors_from_delays(htau.numpy(), w["F"], w["P"])
     t = time.perf_counter()
     O.beamform_channelize_detect(x[:, :1], ph[:, :, :1], w["R"], w["I"])
     one = max(time.perf_counter() - t, 1e-3)
@@ -739,7 +918,7 @@ def run_reference(args):
         "metric": METRIC,
         "value": value,
         "unit": "TMAC/s",
-        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": ms,
@@ -748,13 +927,11 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded CI8 sigma 8, delays U[-5us,5us]); no dataset",
-        "config": {"workload": "ATA production chain: A=28 F=192 T=8192 P=2 B=16, Cast->Beamformer->"
-                               "Channelizer(rate 4)->Detector(Stokes-I, I=4)",
-                   "parallelism": "host cores"},
-        "cpu_baseline": {"value": value, "unit": "TMAC/s", "cores": cores, "kind": "port",
-                         "sample": f"{nch} of {w['F']} channels per step: the reference's numpy test formulas "
-                                   "(tests/modules/beamformer/ata.py, channelizer/advanced.py, "
-                                   "detector/single_pol.py) in FP64"},
+        "config": bench_config(world),
+        "cpu_baseline": {"value": value, "unit": "TMAC/s", "cores": CORES, "kind": "port",
+                         "threads": thread_settings(),
+                         "sample": f"{nch} of {w['F']} channels per step, a per-channel rate: the reference's numpy "
+                                   "test formulas (tests/modules/beamformer/ata.py, detector/single_pol.py) in FP64"},
         "e2e": {"value": value, "unit": "TMAC/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -767,7 +944,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-extra", action="store_true",
-                    help="skip the spectrometer, small-block latency and adjoint legs")
+                    help="skip the spectrometer, latency, adjoint, ModeB, copy and channelizer legs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

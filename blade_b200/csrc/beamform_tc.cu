@@ -86,6 +86,7 @@ struct TcArgs {
     uint32_t raw_tiles, raw_row;  // tiles per raw stage (1, 2 or 4) and its antenna row stride (raw_tiles * 512)
     uint64_t total_tiles;
     uint32_t pdl;  // launched as a programmatic dependent of the phasor split: wait for it before the image
+    uint32_t direct;  // R = 1 CI8 without a raw ring: converter threads load the voltages themselves
 };
 
 __device__ __forceinline__ uint32_t cvt_pair(uint32_t v) {
@@ -396,6 +397,132 @@ __device__ __forceinline__ void build_operand_h16_pair(const uint8_t* raw, uint3
     }
 }
 
+// R = 1 CI8, both polarisations of a tile in one pass.  Thread (converter warp w,
+// lane l) owns samples 4l .. 4l + 3 (rows of the operand) and one group g of 8
+// antennas, fixed for the whole kernel:
+//   KA = 64: g = (l + w) & 7,         warps 0-7;
+//   KA = 32: g = ((l >> 1) + w) & 3,  warps 0-3 (warps 4-7 only keep the handshakes).
+// Loads: one 16-byte load per antenna (4 samples x [p0 re, p0 im, p1 re, p1 im]);
+// the 8 lanes of a quarter-warp read 8 consecutive 16-byte slots of a row, so each
+// is one wavefront.  Stores: a 16-byte chunk of row 4l + j holds 8 antennas of one
+// component; its bank group is g ^ (row & 7) = g ^ 4 (l & 1) ^ j, which the
+// mappings above make distinct over every quarter-warp.  Conversion: byte permutes
+// gather one component of two antennas ([a p0, b p0, a p1, b p1]), the XOR with
+// 0x80 per byte and a second permute with the 0x64 exponent byte give the half2
+// (1024 + x + 128) per polarisation, and one subtraction of 1152 makes it exact x.
+struct R1Task {
+    uint32_t raw_off;        // 8 g * rrow + 16 l in the raw tile
+    uint32_t o_r[4], o_i[4];  // operand offsets of (row 4l + j, K = 8 g) and (row 4l + j, K = KA + 8 g)
+    uint32_t nvalid;         // antennas 8 g .. 8 g + nvalid - 1 exist (0..8)
+    uint32_t active;
+};
+
+__device__ __forceinline__ R1Task r1_task(uint32_t w, uint32_t l, uint32_t A, uint32_t KA, uint32_t rrow) {
+    R1Task t;
+    const uint32_t ng = KA / 8;
+    const uint32_t g = ng == 8 ? ((l + w) & 7u) : (((l >> 1) + w) & 3u);
+    t.active = w < ng;
+    t.raw_off = 8u * g * rrow + 16u * l;
+    const uint32_t a0 = 8u * g;
+    t.nvalid = (t.active && a0 < A) ? min(8u, A - a0) : 0u;
+#pragma unroll
+    for (uint32_t j = 0; j < 4; j++) {
+        t.o_r[j] = op_off(4u * l + j, a0);
+        t.o_i[j] = op_off(4u * l + j, KA + a0);
+    }
+    return t;
+}
+
+// One sample of 8 antennas -> the (re, im) chunks of both polarisations (exact
+// int8 -> FP16; see the R1Task comment).
+__device__ __forceinline__ void r1_convert_store(const uint32_t (&wv)[8], uint8_t* op0, uint8_t* op1, uint32_t o_r,
+                                                 uint32_t o_i) {
+    const half2 h1152 = __halves2half2(__ushort_as_half(0x6480), __ushort_as_half(0x6480));
+    uint32_t r0[4], i0[4], r1[4], i1[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const uint32_t tr = __byte_perm(wv[2 * q], wv[2 * q + 1], 0x6240) ^ 0x80808080u;
+        const uint32_t ti = __byte_perm(wv[2 * q], wv[2 * q + 1], 0x7351) ^ 0x80808080u;
+        r0[q] = h2u(__hsub2(u2h(__byte_perm(tr, 0x64646464u, 0x4140)), h1152));
+        r1[q] = h2u(__hsub2(u2h(__byte_perm(tr, 0x64646464u, 0x4342)), h1152));
+        i0[q] = h2u(__hsub2(u2h(__byte_perm(ti, 0x64646464u, 0x4140)), h1152));
+        i1[q] = h2u(__hsub2(u2h(__byte_perm(ti, 0x64646464u, 0x4342)), h1152));
+    }
+    *reinterpret_cast<uint4*>(op0 + o_r) = make_uint4(r0[0], r0[1], r0[2], r0[3]);
+    *reinterpret_cast<uint4*>(op0 + o_i) = make_uint4(i0[0], i0[1], i0[2], i0[3]);
+    *reinterpret_cast<uint4*>(op1 + o_r) = make_uint4(r1[0], r1[1], r1[2], r1[3]);
+    *reinterpret_cast<uint4*>(op1 + o_i) = make_uint4(i1[0], i1[1], i1[2], i1[3]);
+}
+
+__device__ __forceinline__ void r1_pair_task(const uint8_t* raw, uint32_t rrow, uint8_t* op0, uint8_t* op1,
+                                             const R1Task& t) {
+    if (!t.active) return;
+    const uint8_t* src = raw + t.raw_off;
+    uint4 v[8];
+#pragma unroll
+    for (uint32_t i = 0; i < 8; i++)
+        v[i] = i < t.nvalid ? *reinterpret_cast<const uint4*>(src + i * rrow) : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        uint32_t wv[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) wv[i] = j == 0 ? v[i].x : j == 1 ? v[i].y : j == 2 ? v[i].z : v[i].w;
+        r1_convert_store(wv, op0, op1, t.o_r[j], t.o_i[j]);
+    }
+}
+
+// R = 1 CI8 "direct" mode (no raw ring in shared memory, which leaves room for
+// four operand stages beside a large phasor image): each converter thread loads
+// its voltage words from global memory itself, one tile ahead of the one it
+// builds.  Thread (converter warp w, lane l) owns antenna group g of 8 and the
+// rows l + 32 j (j in its set of sample quarters), fixed for the kernel:
+//   KA = 64: g = w, j = 0..3;   KA = 32: g = w & 3, j = 2 (w >> 2) and 2 (w >> 2) + 1.
+// Loads: 4-byte words, consecutive lanes at consecutive samples of one antenna
+// (128 contiguous bytes per warp load).  Stores: the 16-byte chunk (row l + 32 j,
+// group g) has bank group g ^ (l & 7), distinct over a quarter-warp.
+constexpr uint32_t kDirectMaxJ = 4;
+
+struct DirectTask {
+    uint32_t a0, nvalid, j0, nj;
+    uint32_t o_r[kDirectMaxJ], o_i[kDirectMaxJ];  // offsets of (row l + 32 (j0 + j), K = a0) and (..., K = KA + a0)
+};
+
+__device__ __forceinline__ DirectTask direct_task(uint32_t w, uint32_t l, uint32_t A, uint32_t KA) {
+    DirectTask t;
+    const bool wide = KA == 64;
+    const uint32_t g = wide ? w : (w & 3u);
+    t.j0 = wide ? 0u : 2u * (w >> 2);
+    t.nj = wide ? 4u : 2u;
+    t.a0 = 8u * g;
+    t.nvalid = t.a0 < A ? min(8u, A - t.a0) : 0u;
+#pragma unroll
+    for (uint32_t j = 0; j < kDirectMaxJ; j++) {
+        const uint32_t row = l + 32u * (t.j0 + (j < t.nj ? j : 0u));
+        t.o_r[j] = op_off(row, t.a0);
+        t.o_i[j] = op_off(row, KA + t.a0);
+    }
+    return t;
+}
+
+// The words [j][i] = sample (t0 + l + 32 (j0 + j)) of antenna a0 + i in channel f.
+__device__ __forceinline__ void direct_load(const uint32_t* in, uint32_t F, uint32_t T, uint32_t f, uint32_t t0,
+                                            uint32_t l, const DirectTask& t, uint32_t (&v)[kDirectMaxJ][8]) {
+#pragma unroll
+    for (uint32_t i = 0; i < 8; i++) {
+        const uint32_t* row = in + ((uint64_t)(t.a0 + i) * F + f) * T + t0 + l + 32u * t.j0;
+#pragma unroll
+        for (uint32_t j = 0; j < kDirectMaxJ; j++)
+            v[j][i] = (i < t.nvalid && j < t.nj) ? __ldg(row + 32u * j) : 0u;
+    }
+}
+
+__device__ __forceinline__ void direct_build(const uint32_t (&v)[kDirectMaxJ][8], uint8_t* op0, uint8_t* op1,
+                                             const DirectTask& t) {
+#pragma unroll
+    for (uint32_t j = 0; j < kDirectMaxJ; j++)
+        if (j < t.nj) r1_convert_store(v[j], op0, op1, t.o_r[j], t.o_i[j]);
+}
+
 // Both polarisations of one tile for R = 1 and 2: two single-polarisation passes.
 template <int R>
 __device__ __forceinline__ void build_operand_pair(const uint8_t* raw, uint32_t rrow, uint8_t* op0, uint8_t* op1, uint32_t A,
@@ -640,7 +767,31 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
         }
     } else if (warp == 1) {
         // ---------------- loader: phasor image + raw CI8 tiles (bulk copies) ----------------
-        if (L0 < L1) {
+        if (L0 < L1 && g.direct) {
+            // direct mode: the converter threads load the voltages; only the images here
+            uint32_t wph = 0;
+            bool w_issued = false;
+            uint32_t f = (uint32_t)(L0 / tpc);
+            for (uint64_t L = L0; L < L1; L = (uint64_t)(++f) * tpc) {
+                int ok = 1;
+                if (lane == 0) {
+                    if (g.pdl && L == L0) asm volatile("griddepcontrol.wait;" ::: "memory");
+                    ok = mbar_wait(w_empty, wph ^ 1, abort, kWaitBudget);
+                    if (ok) {
+                        mbar_arrive_expect_tx(w_full, g.img_bytes);
+                        bulk_g2s(w_smem, g.plan + (uint64_t)f * g.img_bytes, g.img_bytes, w_full);
+                    } else {
+                        record_abort(abort, 5);
+                    }
+                }
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                if (!ok) break;
+                w_issued = true;
+                wph ^= 1;
+            }
+            if (lane == 0 && w_issued && !mbar_wait(w_full, wph ^ 1, &never, kWaitBudget)) record_abort(abort, 6);
+            __syncwarp();
+        } else if (L0 < L1) {
             uint32_t rs = 0, rph = 0, wph = 0;
             bool w_issued = false;
             uint32_t issued_mask = 0, issued_par = 0;  // per raw stage: issued?, parity of last issue
@@ -816,7 +967,44 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
                 }
             }
         }
-        if (!(R == 4 && split)) {
+        if constexpr (R == 1 && ES == 4) {
+            if (g.direct) {
+                // Pair mode without a raw ring: registers hold this tile's words, loaded
+                // while the previous tile was built; the next tile's loads go out first.
+                const DirectTask dt = direct_task(ct >> 5, lane, g.A, KA);
+                const uint32_t* in32 = reinterpret_cast<const uint32_t*>(g.in);
+                uint32_t va[kDirectMaxJ][8], vb[kDirectMaxJ][8];
+                uint32_t f = (uint32_t)(L0 / tpc), tt = (uint32_t)(L0 % tpc);
+                if (L0 < L1) direct_load(in32, g.F, g.T, f, tt * kM, lane, dt, va);
+                uint32_t as = 0, aph = 0;
+                for (uint64_t L = L0; L < L1; L += 2) {
+                    // tile L from va (tile L + 1 into vb first), then tile L + 1 from vb
+                    // (tile L + 2 into va first)
+#pragma unroll
+                    for (int half = 0; half < 2; half++) {
+                        if (half == 1 && L + 1 >= L1) break;
+                        uint32_t nf = f, ntt = tt + 1;
+                        if (ntt == tpc) { ntt = 0; nf++; }
+                        if (L + half + 1 < L1) direct_load(in32, g.F, g.T, nf, ntt * kM, lane, dt, half ? va : vb);
+                        if (!mbar_wait(&a_empty[as + 1], aph ^ 1, abort, kWaitBudget)) {
+                            record_abort(abort, 8);
+                            L = L1;
+                            break;
+                        }
+                        uint8_t* op0 = a_smem + (size_t)as * op_bytes;
+                        direct_build(half ? vb : va, op0, op0 + op_bytes, dt);
+                        fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&a_full[as + 1]);
+                        as += 2;
+                        if (as == AS) { as = 0; aph ^= 1; }
+                        f = nf;
+                        tt = ntt;
+                    }
+                }
+            }
+        }
+        if (!(R == 4 && split) && !g.direct) {
         // R = 4 pair mode: this warp's warp-tasks (KA / 4 of them over kConvWarps warps),
         // addresses fixed for the kernel
         constexpr uint32_t kMaxT4 = kMaxKA / 4 / kConvWarps;
@@ -826,6 +1014,8 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
 #pragma unroll
             for (uint32_t i = 0; i < kMaxT4; i++) t4[i] = r4_task((ct >> 5) + i * kConvWarps, lane, g.A, KA, g.raw_row);
         }
+        R1Task t1;
+        if constexpr (R == 1 && ES == 4) t1 = r1_task(ct >> 5, lane, g.A, KA, g.raw_row);
         uint32_t rs = 0, rph = 0, as = 0, aph = 0;
         uint32_t sub = 0;  // tile within the raw stage (CTA ranges are stage-aligned)
         bool ok = true;
@@ -850,6 +1040,8 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
                         if (i < nt4) r4_pair_task(raw, g.raw_row, op0, op1, t4[i]);
                 } else if constexpr (ES == 8) {
                     build_operand_h16_pair(raw, g.raw_row, op0, op1, g.A, KA, ct);
+                } else if constexpr (R == 1) {
+                    r1_pair_task(raw, g.raw_row, op0, op1, t1);
                 } else {
                     build_operand_pair<R>(raw, g.raw_row, op0, op1, g.A, KA, ct);
                 }
@@ -992,12 +1184,13 @@ __global__ void __launch_bounds__(256) tc_prepare_kernel(const float2* __restric
 
 struct TcShape {
     uint32_t NB, KA, nchunks, img_bytes, raw_bytes, a_stages, r_stages, stacked;
-    uint32_t raw_tiles, raw_row;
+    uint32_t raw_tiles, raw_row, direct;
     size_t smem;
 };
 
 // T = 0 sizes only the phasor image (the ring layout needs the tiles per channel).
-bool tc_shape(uint64_t B, uint64_t A, TcShape& s, uint64_t T = 0, uint32_t es = 4) {
+bool tc_shape(uint64_t B, uint64_t A, TcShape& s, uint64_t T = 0, uint32_t es = 4, uint64_t rate = 0) {
+    s.direct = 0;
     if (A == 0 || A > kMaxKA || B == 0) return false;
     const uint64_t bc = B < (uint64_t)kMaxNB ? B : (uint64_t)kMaxNB;
     s.NB = (uint32_t)((bc + 15) / 16 * 16);
@@ -1064,6 +1257,22 @@ bool tc_shape(uint64_t B, uint64_t A, TcShape& s, uint64_t T = 0, uint32_t es = 
     s.a_stages = as;
     s.r_stages = rs;
     s.smem = fixed + as * op + rs * (size_t)s.raw_bytes;
+    if (T && es == 4 && rate == 1 && as < 4) {
+        // A phasor image this large leaves no room for a raw ring and a build-ahead
+        // operand ring together: at rate 1 the converter threads load the voltages
+        // themselves and the shared memory holds operand tile pairs only (two pairs
+        // at least, so that the build runs a tile ahead and two issuers alternate).
+        for (uint32_t c : {8u, 4u}) {
+            if (fixed + c * op <= limit) {
+                s.direct = 1;
+                s.a_stages = c;
+                s.r_stages = 0;
+                s.raw_bytes = 0;
+                s.smem = fixed + c * op;
+                return true;
+            }
+        }
+    }
     return true;
 }
 
@@ -1167,7 +1376,7 @@ int tc_run(const char* who, const void* in, const void* plan, void* out, uint64_
            uint64_t T, uint64_t rate, uint64_t integration, uint32_t es, TcKernel fn, blade_stream_t stream,
            bool pdl = false) {
     TcShape s;
-    tc_shape(B, A, s, T, es);
+    tc_shape(B, A, s, T, es, rate);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (int rc = ensure_smem(reinterpret_cast<const void*>(fn), s.smem)) return rc;
     const uint32_t U = (uint32_t)(T / (rate * integration));
@@ -1196,6 +1405,7 @@ int tc_run(const char* who, const void* in, const void* plan, void* out, uint64_
         g.tiles_per_ch = (uint32_t)(T / kM);
         g.total_tiles = (uint64_t)F * (T / kM);
         g.pdl = (pdl && c == 0) ? 1u : 0u;
+        g.direct = s.direct;
         // Whole raw stages per CTA (the kernel rounds its share up to raw_tiles); no
         // CTA is left without tiles.
         const uint64_t sms = (uint64_t)sm_count();
@@ -1334,21 +1544,50 @@ namespace {
 
 constexpr uint64_t kNoAllocPlanBytes = 8ull << 20;
 
-// Device address of g_tc_noalloc_plan, looked up once per device with that device
-// current (the host-side name is only a stand-in for the device array).
+template <typename Fn>
+int driver_entry(const char* name, unsigned version, Fn* fn) {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPointByVersion(name, &p, version, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p)
+        return set_error(BLADE_CUDA_ERROR, "blade_beamform_detect_tc_noalloc: %s unavailable", name);
+    *fn = reinterpret_cast<Fn>(p);
+    return BLADE_SUCCESS;
+}
+
+// Device address of g_tc_noalloc_plan, looked up with the device current (the
+// host-side name is only a stand-in for the device array) once per device and
+// context: the cache is keyed on the current context's unique id as well, so
+// after a cudaDeviceReset, which destroys the primary context and this module's
+// copy of the array with it, the next call looks the address up again.
 int noalloc_plan_address(void** out) {
     static std::mutex mu;
     static void* addr[64] = {nullptr};
+    static unsigned long long ctx_of[64] = {0};
+    static PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
+    static PFN_cuCtxGetId_v12000 get_id = nullptr;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return check_cuda(e, "blade_beamform_detect_tc_noalloc");
     if (dev < 0 || dev >= 64) return set_error(BLADE_ERROR, "blade_beamform_detect_tc_noalloc: device %d", dev);
+    // makes the device's primary context current, creating it if a reset destroyed it
+    e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return check_cuda(e, "blade_beamform_detect_tc_noalloc: cudaSetDevice");
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
+    if (!get_current) {
+        if (int rc = driver_entry("cuCtxGetCurrent", 4000, &get_current)) return rc;
+        if (int rc = driver_entry("cuCtxGetId", 12000, &get_id)) return rc;
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        return set_error(BLADE_CUDA_ERROR, "blade_beamform_detect_tc_noalloc: no current CUDA context");
+    if (!addr[dev] || ctx_of[dev] != id) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_tc_noalloc_plan);
         if (e != cudaSuccess) return check_cuda(e, "blade_beamform_detect_tc_noalloc: cudaGetSymbolAddress");
         addr[dev] = p;
+        ctx_of[dev] = id;
     }
     *out = addr[dev];
     return BLADE_SUCCESS;

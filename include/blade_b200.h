@@ -307,10 +307,14 @@ BLADE_API int blade_device_status(uint32_t* status);
  * fixed-cadence loop cannot absorb the device synchronisation of an allocation.
  * Limit: blade_beamform_tc_plan_size(B, A, F, P) <= 8 MiB (e.g. A <= 32,
  * B <= 16 up to 512 channels); larger images are rejected with BLADE_ERROR.
- * The first call on each device looks up the array's device address (make that
- * first call before any stream capture).  All calls share the one array: calls
- * that overlap on the GPU (different streams, or different host threads) race;
- * serialise them on one stream.  Each call rewrites the whole image it uses.
+ * The array is part of the library's device code: every process that loads
+ * the library holds these 8 MiB on each device it uses, from the module load
+ * until exit, whether or not it ever calls this function.
+ * The first call on each device (and the first after a cudaDeviceReset) looks
+ * up the array's device address (make that first call before any stream
+ * capture).  All calls share the one array: calls that overlap on the GPU
+ * (different streams, or different host threads) race; serialise them on one
+ * stream.  Each call rewrites the whole image it uses.
  * ------------------------------------------------------------------------- */
 BLADE_API int blade_beamform_detect_tc_noalloc(const void* in, const void* phasors,
                                                void* out, uint64_t B, uint64_t A,

@@ -1,6 +1,6 @@
 """Runs one hot-path kernel on one workload a few times, for profilers.
 
-    python -m blade_b200.profile_case --workload ata-production --path tc --launches 4
+    python profile_case.py --workload ata-production --path tc --launches 4
 
 Workloads: ata-small (A=20 F=96 T=256 B=8 rate 1 I=4), ata-production
 (A=28 F=192 T=8192 B=16 rate 4 I=4), dense-64x64 (A=64 F=256 T=8192 B=64 rate 1
@@ -22,8 +22,8 @@ import argparse
 
 import torch
 
-from . import _lib
-from .synthetic import DF_HZ, F0_HZ
+from blade_b200 import _lib
+from blade_b200.synthetic import DF_HZ, F0_HZ
 
 WORKLOADS = {
     "ata-small": dict(A=20, F=96, T=256, B=8, R=1, I=4),

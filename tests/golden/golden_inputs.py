@@ -63,3 +63,41 @@ def det_input():
 
 def ch_input():
     return complex_ints((CH["A"], CH["F"], CH["T"], 2), 41)
+
+
+# Byte-movement and polarizer fixtures (the reference's device-only kernels,
+# oracle/_ref/ref_*.cubin).  Polarizer inputs have 24-bit fractions, so its sums
+# round and bit equality is a real check of the arithmetic.
+POL_SHAPE = (2, 4, 64, 2)                      # Polarizer [A, F, T, P], CF32 and CF16
+GATHER_CASES = [((2, 3, 8, 2), 2, 4),          # (input shape, axis, multiplier); all widths
+                ((2, 3, 8, 2), 1, 3),          # below the reference's 512-element copy
+                ((3, 2, 4, 2), 0, 2)]          # threshold, so its accumulate kernel runs
+PERM_SHAPE = (2, 3, 5, 2)
+PERMS = [(0, 2, 1, 3), (0, 2, 3, 1), (3, 2, 1, 0)]
+
+
+def complex_frac(shape, seed) -> np.ndarray:
+    """complex64 with re, im = k / 2^23 - 1 for 24-bit k (exact in FP32)."""
+    n = int(np.prod(shape))
+    k = (lcg(2 * n, seed) >> np.uint32(8)).astype(np.float64)
+    v = (k / 2.0 ** 23 - 1.0).astype(np.float32).reshape(tuple(shape) + (2,))
+    return (v[..., 0] + 1j * v[..., 1]).astype(np.complex64)
+
+
+def pol_input_cf32() -> np.ndarray:
+    return complex_frac(POL_SHAPE, 51)
+
+
+def pol_input_cf16() -> np.ndarray:
+    """float16 [..., 2] (re, im) pairs: the CF16 layout."""
+    x = complex_frac(POL_SHAPE, 52)
+    return np.stack([x.real, x.imag], axis=-1).astype(np.float16)
+
+
+def gather_inputs(case: int):
+    shape, _, mult = GATHER_CASES[case]
+    return [complex_frac(shape, 60 + 10 * case + k) for k in range(mult)]
+
+
+def perm_input() -> np.ndarray:
+    return complex_frac(PERM_SHAPE, 71)

@@ -1,6 +1,7 @@
 """Regenerates tests/golden/reference_kernels.npz: the outputs of the reference's own
-CUDA kernels (oracle/_ref/libref_kernels.so, built from the reference sources by
-oracle/ref_kernels/build.sh) on the deterministic inputs of golden_inputs.py.
+CUDA kernels (oracle/_ref/libref_kernels.so and the device-only oracle/_ref/ref_*.cubin,
+built from the reference sources by oracle/ref_kernels/build.sh) on the
+deterministic inputs of golden_inputs.py.
 
 Needs a GPU.  Usage:  python tests/golden/make_golden.py [output.npz]
 """
@@ -15,6 +16,7 @@ import torch
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, HERE)
+sys.path.insert(0, ROOT)
 
 import golden_inputs as G  # noqa: E402
 
@@ -57,6 +59,39 @@ def main(out_path):
     assert lib.ref_channelizer(ctypes.c_void_p(xd.data_ptr())) == 0
     A, F, T = G.CH["A"], G.CH["F"], G.CH["T"]
     res["channelizer_rate_T"] = xd.cpu().numpy().reshape(A, F * T, 1, 2)
+
+    # device-only kernels (polarizer, gather's accumulate, permutation), launched
+    # with the reference modules' geometry: PadGridSize(input size, 512) x 512
+    from oracle.ref_kernels import cubin as RK
+
+    for key, x in (("polarizer_cf32", G.pol_input_cf32()), ("polarizer_cf16", G.pol_input_cf16())):
+        k = RK.Kernel(key)
+        xd = dev(x)
+        v = RK.ref_vector(xd.data_ptr(), G.POL_SHAPE)  # in place: the module links its output to its input
+        k.launch(RK.pad_grid(int(np.prod(G.POL_SHAPE)), 512), 512, v, v)
+        res[key] = xd.cpu().numpy()
+
+    k = RK.Kernel("gather_cf32")
+    for c, (shape, axis, mult) in enumerate(G.GATHER_CASES):
+        oshape = list(shape)
+        oshape[axis] *= mult
+        od = torch.zeros(oshape, dtype=torch.complex64, device="cuda")
+        ov = RK.ref_vector(od.data_ptr(), oshape)
+        for step, x in enumerate(G.gather_inputs(c)):
+            xd = dev(x)
+            k.launch(RK.pad_grid(x.size, 512), 512, RK.ref_vector(xd.data_ptr(), shape), ov,
+                     ctypes.c_uint64(axis), ctypes.c_uint64(step * shape[axis]))
+        res[f"gather_case{c}"] = od.cpu().numpy()
+
+    k = RK.Kernel("permutation_cf32")
+    x = G.perm_input()
+    xd = dev(x)
+    for idx in G.PERMS:
+        oshape = [G.PERM_SHAPE[i] for i in idx]
+        od = torch.zeros(oshape, dtype=torch.complex64, device="cuda")
+        k.launch(RK.pad_grid(x.size, 512), 512, RK.ref_vector(xd.data_ptr(), G.PERM_SHAPE),
+                 RK.ref_vector(od.data_ptr(), oshape), RK.ref_shape(idx))
+        res["permute_" + "".join(map(str, idx))] = od.cpu().numpy()
 
     np.savez_compressed(out_path, **res)
     print("wrote", out_path, {k: v.shape for k, v in res.items()})

@@ -30,6 +30,11 @@ CHAINS = [
     ("tmem-operand-5ant", 5, 3, 256, 3, 4, 1),
     ("tmem-operand-32ant", 32, 2, 1024, 16, 4, 32),
     ("tmem-operand-i8", 17, 5, 2048, 9, 4, 8),
+    # rate 1 with a large phasor image (converters load the voltages directly): ragged
+    # antennas and an odd number of tiles per CTA, 48 beams (padded rows), two beam chunks
+    ("direct-ragged", 50, 40, 1152, 64, 1, 4),
+    ("direct-48-beams", 64, 4, 2048, 48, 1, 16),
+    ("direct-two-chunks", 64, 3, 1024, 100, 1, 8),
 ]
 
 
@@ -73,7 +78,7 @@ def test_tensor_core_chain(cuda, name, A, F, T, B, R, I):
     np.testing.assert_array_equal(host(od2), y)
 
 
-@pytest.mark.parametrize("name,A,F,T,B,R,I", [CHAINS[1], CHAINS[4], CHAINS[5]])
+@pytest.mark.parametrize("name,A,F,T,B,R,I", [CHAINS[1], CHAINS[4], CHAINS[5], CHAINS[10]])
 def test_prepare_detect_tc_matches_two_calls(cuda, name, A, F, T, B, R, I):
     # the chain launched as a programmatic dependent of the split must read the
     # split's new image, never the plan's previous contents: each call below

@@ -3,9 +3,10 @@ reference sources, oracle/ref_kernels) on deterministic inputs, committed in
 tests/golden/reference_kernels.npz by tests/golden/make_golden.py.
 
 CPU: pins the FP64 oracle to the reference kernels.  GPU: our kernels against
-the same fixtures.  Cast is compared bit for bit; the FP32 kernels within the
-relative-L2 bound (the reference's detector sums with atomicAdd in arbitrary
-order, and cuFFT's rounding differs from the Stockham FFT's)."""
+the same fixtures.  Cast, Polarizer, Gather and Permutation are compared bit for
+bit; the FP32 kernels within the relative-L2 bound (the reference's detector sums
+with atomicAdd in arbitrary order, and cuFFT's rounding differs from the Stockham
+FFT's)."""
 
 import os
 import sys
@@ -58,7 +59,82 @@ def test_oracle_channelizer_matches_reference_kernel(gold):
     assert rel(O.channelize(x, G.CH["T"]), gold["channelizer_rate_T"]) < TOL
 
 
+def need(gold, *keys):
+    missing = [k for k in keys if k not in gold]
+    if missing:
+        pytest.skip(f"golden fixture lacks {missing}: rerun tests/golden/make_golden.py on a GPU")
+
+
+def cf16_to_complex(h):
+    return h[..., 0].astype(np.float64) + 1j * h[..., 1].astype(np.float64)
+
+
+def complex_to_cf16(y):
+    return np.stack([y.real, y.imag], axis=-1).astype(np.float16)
+
+
+def test_oracle_polarizer_matches_reference_kernel(gold):
+    need(gold, "polarizer_cf32", "polarizer_cf16")
+    # FP64 sums of two FP32 (FP16) values are exact here, so rounding them once
+    # gives the correctly rounded FP32 (FP16) sums the kernel must produce
+    np.testing.assert_array_equal(O.polarize(G.pol_input_cf32()).astype(np.complex64), gold["polarizer_cf32"])
+    np.testing.assert_array_equal(complex_to_cf16(O.polarize(cf16_to_complex(G.pol_input_cf16()))),
+                                  gold["polarizer_cf16"])
+
+
+def test_oracle_gather_matches_reference_kernel(gold):
+    need(gold, *[f"gather_case{c}" for c in range(len(G.GATHER_CASES))])
+    for c, (_, axis, _) in enumerate(G.GATHER_CASES):
+        np.testing.assert_array_equal(O.gather(G.gather_inputs(c), axis), gold[f"gather_case{c}"])
+
+
+def test_oracle_permutation_matches_reference_kernel(gold):
+    keys = ["permute_" + "".join(map(str, idx)) for idx in G.PERMS]
+    need(gold, *keys)
+    x = G.perm_input()
+    for idx, key in zip(G.PERMS, keys):
+        np.testing.assert_array_equal(O.permute(x, idx), gold[key])
+
+
 # ----------------------------------------------------------------------------- GPU: our kernels vs reference kernels
+@pytest.mark.gpu
+def test_byte_kernels_match_reference_kernels(cuda, gold):
+    """Polarizer (CF32, CF16), Gather (CHRONOUS, every step) and Permutation against
+    the reference's own kernels, bit for bit."""
+    import torch
+
+    from blade_b200 import _lib
+    from tests.gpu_util import call, dev, host, ptr, stream
+
+    perm_keys = ["permute_" + "".join(map(str, idx)) for idx in G.PERMS]
+    need(gold, "polarizer_cf32", "polarizer_cf16", *perm_keys,
+         *[f"gather_case{c}" for c in range(len(G.GATHER_CASES))])
+    n = int(np.prod(G.POL_SHAPE[:3]))  # dual-polarisation samples
+    for key, x, code in (("polarizer_cf32", G.pol_input_cf32(), _lib.CF32),
+                         ("polarizer_cf16", G.pol_input_cf16(), _lib.CF16)):
+        xd = dev(x)
+        call("blade_polarize", code, ptr(xd), ptr(xd), n, stream())
+        np.testing.assert_array_equal(host(xd), gold[key])
+
+    for c, (shape, axis, mult) in enumerate(G.GATHER_CASES):
+        oshape = list(shape)
+        oshape[axis] *= mult
+        od = torch.zeros(oshape, dtype=torch.complex64, device="cuda")
+        for step, x in enumerate(G.gather_inputs(c)):
+            xd = dev(x)
+            call("blade_gather", 8, ptr(xd), ptr(od), _lib.u64_array(shape), axis, mult, step, stream())
+            torch.cuda.synchronize()
+        np.testing.assert_array_equal(host(od), gold[f"gather_case{c}"])
+
+    x = G.perm_input()
+    xd = dev(x)
+    for idx, key in zip(G.PERMS, perm_keys):
+        od = torch.zeros([G.PERM_SHAPE[i] for i in idx], dtype=torch.complex64, device="cuda")
+        call("blade_permute", 8, ptr(xd), ptr(od), _lib.u64_array(G.PERM_SHAPE), _lib.u64_array(idx), stream())
+        np.testing.assert_array_equal(host(od), gold[key])
+
+
+# ----------------------------------------------------------------------------- GPU: our kernels vs reference kernels (FP32)
 @pytest.mark.gpu
 def test_kernels_match_reference_kernels(cuda, gold):
     import torch
