@@ -18,7 +18,7 @@ The compute path is ``libblade_b200.so`` (hand-written sm_100a CUDA behind a C
 ABI, include/blade_b200.h); PyTorch only supplies device memory and streams.
 """
 
-from . import _lib
+from . import _lib, autotune
 from .constants import *  # noqa: F401,F403  (bl.cf32, bl.ata, bl.beamformer, bl.pol, bl.result, ...)
 from .constants import Constant, Taint, pol, result
 from .memory import Duet, Vector, array_tensor, delay_tensor, phasor_tensor, tensor

@@ -67,6 +67,11 @@ _SIGNATURES = {
     "blade_beamform_detect_adjoint": (_int, [_vp, _vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp]),
     "blade_device_status": (_int, [C.POINTER(C.c_uint32)]),
     "blade_beamform_detect_tc_noalloc": (_int, [_vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),
+    "blade_beamform_detect_tc_autotune": (_int, [_u64, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),
+    "blade_beamform_detect_f32_autotune": (_int, [_int, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),
+    "blade_spectrometer_autotune": (_int, [_int, _int, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),
+    "blade_autotune_query": (_int, [_int, _u64p, C.POINTER(C.c_uint32), C.POINTER(C.c_float), C.POINTER(_int)]),
+    "blade_autotune_clear": (_int, []),
 }
 
 

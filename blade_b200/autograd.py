@@ -10,7 +10,9 @@ and never stores them.  PyTorch's complex-gradient convention
 (grad = dL/dRe w + i dL/dIm w = 2 dL/d conj(w)) is applied in ``backward``.
 
 ``calibrate_phases`` runs gradient ascent on the summed Stokes-I of a boresight
-beam over per-antenna phases, the gain/phase calibration use of the adjoint.
+beam over per-antenna phases; ``calibrate_gains`` over unit-norm complex weights,
+which recovers both the relative gain magnitudes and the phases: the gain/phase
+calibration use of the adjoint.
 """
 
 from __future__ import annotations
@@ -80,3 +82,30 @@ def calibrate_phases(x: torch.Tensor, steps: int = 200, lr: float = 0.05, ref: i
     with torch.no_grad():
         rel = theta - theta[ref]
         return torch.remainder(rel + math.pi, 2 * math.pi) - math.pi
+
+
+def calibrate_gains(x: torch.Tensor, steps: int = 300, lr: float = 0.05, ref: int = 0):
+    """Per-antenna gain and phase calibration of a boresight beam by gradient ascent
+    on its summed Stokes-I over complex weights of unit norm, w = u / |u| with
+    w[0, a, f, 0, p] = w_a (Adam on u).  For voltages v_a = g_a exp(i phi_a) s + n_a
+    with equal noise powers the power sum_{f,t,p} |sum_a v_a w_a|^2 is a Rayleigh
+    quotient whose maximiser is proportional to conj(g_a exp(i phi_a)), so
+    |w_a| / |w_ref| -> |g_a| / |g_ref| and -arg(w_a / w_ref) -> phi_a - phi_ref.
+    Returns (gain ratios |g_a| / |g_ref|, phases relative to antenna ``ref``
+    wrapped to (-pi, pi])."""
+    A, F, T, P = x.shape
+    u = torch.ones(A, dtype=torch.complex64, device=x.device, requires_grad=True)
+    opt = torch.optim.Adam([u], lr=lr)
+    scale = 1.0 / float(F * T * P)
+    for _ in range(steps):
+        opt.zero_grad()
+        wa = u / torch.linalg.vector_norm(u)
+        w = wa.view(1, A, 1, 1, 1).expand(1, A, F, 1, P).contiguous()
+        loss = stokes_loss(x, w) * scale
+        loss.backward()
+        opt.step()
+    with torch.no_grad():
+        wa = u / torch.linalg.vector_norm(u)
+        gains = wa.abs() / wa[ref].abs()
+        rel = -(torch.angle(wa) - torch.angle(wa[ref]))
+        return gains, torch.remainder(rel + math.pi, 2 * math.pi) - math.pi

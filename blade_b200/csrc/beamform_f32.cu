@@ -21,6 +21,7 @@
 // registers (their coefficients are +-1, +-i), |.|^2 is summed over both
 // polarisations, and the integration window is closed with warp shuffles over
 // adjacent lanes.  Nothing but the Stokes-I output touches HBM.
+#include "autotune.cuh"
 #include "common.cuh"
 
 namespace bb {
@@ -434,6 +435,64 @@ extern "C" int blade_beamform_meerkat_f32(const void* in, const void* phasors, v
     return check_launch("blade_beamform_meerkat_f32");
 }
 
+namespace bb {
+
+int f32_default_tg(uint64_t B, uint64_t rate, uint64_t integration) {
+    int tg = pick_tg(B);
+    // The window (rate * integration samples) must tile the CTA's 4 TG samples and
+    // span at most one warp of threads.
+    while (tg < 256 && (4ull * tg) % (rate * integration) != 0) tg *= 2;
+    return tg;
+}
+
+bool f32_tg_ok(uint32_t tg, uint64_t B, uint64_t rate, uint64_t integration) {
+    return (tg == 32 || tg == 64 || tg == 128 || tg == 256) && (4ull * tg) % (rate * integration) == 0 &&
+           ceil_div(B, 1024 / tg) <= 65535;
+}
+
+// TG of a fused FP32 launch: the tuned width for this shape on this device when
+// blade_beamform_detect_f32_autotune stored one, else the default.
+int f32_tg(uint64_t B, uint64_t A, uint64_t F, uint64_t T, uint64_t rate, uint64_t integration, int in_type,
+           bool* tuned = nullptr, TuneEntry* entry = nullptr) {
+    int tg = f32_default_tg(B, rate, integration);
+    if (tuned) *tuned = false;
+    const uint64_t key[8] = {B, A, F, T, 2, rate, integration, (uint64_t)in_type};
+    TuneEntry e;
+    if (tune_lookup(BLADE_TUNE_F32, key, &e) && f32_tg_ok(e.params[0], B, rate, integration)) {
+        tg = (int)e.params[0];
+        if (tuned) *tuned = true;
+        if (entry) *entry = e;
+    }
+    return tg;
+}
+
+void f32_launch(int in_type, int tg, const void* in, const float2* ph, void* out, uint64_t B, uint64_t A, uint64_t F,
+                uint64_t T, uint64_t rate, uint64_t integration, cudaStream_t s) {
+    const PhLayout lay = ata_layout(A, F, 2);
+    if (in_type == BLADE_CI8) {
+        if (rate == 1) dispatch_tg<2, IN_CI8, 1>(tg, in, ph, out, B, A, F, T, integration, s, lay);
+        else if (rate == 2) dispatch_tg<2, IN_CI8, 2>(tg, in, ph, out, B, A, F, T, integration, s, lay);
+        else dispatch_tg<2, IN_CI8, 4>(tg, in, ph, out, B, A, F, T, integration, s, lay);
+    } else {
+        if (rate == 1) dispatch_tg<2, IN_CF32, 1>(tg, in, ph, out, B, A, F, T, integration, s, lay);
+        else if (rate == 2) dispatch_tg<2, IN_CF32, 2>(tg, in, ph, out, B, A, F, T, integration, s, lay);
+        else dispatch_tg<2, IN_CF32, 4>(tg, in, ph, out, B, A, F, T, integration, s, lay);
+    }
+}
+
+int f32_query(const uint64_t (&shape)[8], uint32_t* params, float* us, int* tuned) {
+    bool t = false;
+    TuneEntry e;
+    const int tg = f32_tg(shape[0], shape[1], shape[2], shape[3], shape[5], shape[6], (int)shape[7], &t, &e);
+    for (int i = 0; i < kTuneParams; i++) params[i] = t ? e.params[i] : 0u;
+    params[0] = (uint32_t)tg;
+    *us = t ? e.us : 0.f;
+    *tuned = t ? 1 : 0;
+    return BLADE_SUCCESS;
+}
+
+}  // namespace bb
+
 extern "C" int blade_beamform_detect_f32(int in_type, const void* in, const void* phasors, void* out, uint64_t B,
                                          uint64_t A, uint64_t F, uint64_t T, uint64_t P, uint64_t rate,
                                          uint64_t integration, blade_stream_t stream) {
@@ -450,10 +509,7 @@ extern "C" int blade_beamform_detect_f32(int in_type, const void* in, const void
     if (!in || !phasors || !out) return set_error(BLADE_ERROR, "blade_beamform_detect_f32: null buffer");
     if (!dims_ok(B, A, F, T)) return set_error(BLADE_ERROR, "blade_beamform_detect_f32: dimensions out of range");
     const uint64_t ns = 4 / rate;  // spectra per thread
-    int tg = pick_tg(B);
-    // The window (rate * integration samples) must tile the CTA's 4 TG samples and
-    // span at most one warp of threads.
-    while (tg < 256 && (4ull * tg) % (rate * integration) != 0) tg *= 2;
+    const int tg = f32_tg(B, A, F, T, rate, integration, in_type);
     if ((4ull * tg) % (rate * integration) != 0)
         return set_error(BLADE_ERROR, "blade_beamform_detect_f32: rate * integration must divide %d", 4 * tg);
     if (integration > ns) {
@@ -469,17 +525,84 @@ extern "C" int blade_beamform_detect_f32(int in_type, const void* in, const void
         return set_error(BLADE_ERROR, "blade_beamform_detect_f32: CF32 input must be 16-byte aligned");
     if (in_type == BLADE_CI8 && (reinterpret_cast<uintptr_t>(in) & 3))
         return set_error(BLADE_ERROR, "blade_beamform_detect_f32: CI8 input must be 4-byte aligned");
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const float2* ph = static_cast<const float2*>(phasors);
-    const PhLayout lay = ata_layout(A, F, 2);
-    if (in_type == BLADE_CI8) {
-        if (rate == 1) dispatch_tg<2, IN_CI8, 1>(tg, in, ph, out, B, A, F, T, integration, s, lay);
-        else if (rate == 2) dispatch_tg<2, IN_CI8, 2>(tg, in, ph, out, B, A, F, T, integration, s, lay);
-        else dispatch_tg<2, IN_CI8, 4>(tg, in, ph, out, B, A, F, T, integration, s, lay);
-    } else {
-        if (rate == 1) dispatch_tg<2, IN_CF32, 1>(tg, in, ph, out, B, A, F, T, integration, s, lay);
-        else if (rate == 2) dispatch_tg<2, IN_CF32, 2>(tg, in, ph, out, B, A, F, T, integration, s, lay);
-        else dispatch_tg<2, IN_CF32, 4>(tg, in, ph, out, B, A, F, T, integration, s, lay);
-    }
+    f32_launch(in_type, tg, in, static_cast<const float2*>(phasors), out, B, A, F, T, rate, integration,
+               reinterpret_cast<cudaStream_t>(stream));
     return check_launch("blade_beamform_detect_f32");
+}
+
+extern "C" int blade_beamform_detect_f32_autotune(int in_type, uint64_t B, uint64_t A, uint64_t F, uint64_t T,
+                                                  uint64_t P, uint64_t rate, uint64_t integration,
+                                                  blade_stream_t stream) {
+    using namespace bb;
+    const char* who = "blade_beamform_detect_f32_autotune";
+    if (P != 2 || (rate != 1 && rate != 2 && rate != 4) || integration == 0 || T % (rate * integration) != 0 ||
+        (in_type != BLADE_CF32 && in_type != BLADE_CI8) || B == 0 || A == 0 || F == 0 || T == 0 ||
+        !dims_ok(B, A, F, T))
+        return set_error(BLADE_ERROR, "%s: unsupported configuration", who);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const size_t n = (size_t)A * F * T * P;  // complex samples
+    const size_t in_bytes = n * (in_type == BLADE_CI8 ? 2 : 8), ph_count = (size_t)B * A * F * P;
+    const size_t out_bytes = (size_t)B * F * rate * (T / (rate * integration)) * sizeof(float);
+    std::vector<void*> bufs;
+    auto get = [&](size_t bytes) {
+        void* q = nullptr;
+        if (cudaMalloc(&q, bytes < 16 ? 16 : bytes) != cudaSuccess) return (void*)nullptr;
+        bufs.push_back(q);
+        return q;
+    };
+    struct Free {
+        std::vector<void*>& b;
+        ~Free() {
+            for (void* q : b) cudaFree(q);
+        }
+    } release{bufs};
+    void* in = get(in_bytes);
+    void* ph = get(ph_count * sizeof(float2));
+    void* ref = get(out_bytes);
+    void* out = get(out_bytes);
+    if (!in || !ph || !ref || !out) return set_error(BLADE_CUDA_ERROR, "%s: allocation failed", who);
+    if (in_type == BLADE_CI8) {
+        if (int rc = tune_fill_ci8(in, in_bytes, st)) return rc;
+    } else {
+        if (int rc = tune_fill_phasors(in, n, st)) return rc;  // unit-modulus samples serve as CF32 voltages
+    }
+    if (int rc = tune_fill_phasors(ph, ph_count, st)) return rc;
+    // the public entry validates the configuration (window and rate rules)
+    if (int rc = blade_beamform_detect_f32(in_type, in, ph, ref, B, A, F, T, P, rate, integration, stream)) return rc;
+    const int def = f32_default_tg(B, rate, integration);
+    std::vector<int> cands{def};
+    for (int tg : {32, 64, 128, 256})
+        if (tg != def && f32_tg_ok((uint32_t)tg, B, rate, integration)) cands.push_back(tg);
+    int best = -1;
+    float best_us = 0.f;
+    uint32_t ndiff = 0, ntimed = 0;
+    for (size_t i = 0; i < cands.size(); i++) {
+        void* dst = i == 0 ? ref : out;
+        const float us = tune_time(
+            [&]() {
+                f32_launch(in_type, cands[i], in, static_cast<const float2*>(ph), dst, B, A, F, T, rate, integration,
+                           st);
+                return check_launch(who);
+            },
+            st);
+        if (us < 0.f) return set_error(BLADE_CUDA_ERROR, "%s: candidate TG=%d failed: %s", who, cands[i],
+                                       blade_last_error());
+        ntimed++;
+        if (i > 0 && !tune_same(ref, out, out_bytes)) {
+            ndiff++;
+            continue;
+        }
+        if (best < 0 || us < best_us) {
+            best = (int)i;
+            best_us = us;
+        }
+    }
+    TuneEntry e = {};
+    e.params[0] = (uint32_t)cands[best];
+    e.params[4] = ntimed;
+    e.params[5] = ndiff;
+    e.us = best_us;
+    const uint64_t key[8] = {B, A, F, T, P, rate, integration, (uint64_t)in_type};
+    tune_store(BLADE_TUNE_F32, key, e);
+    return BLADE_SUCCESS;
 }

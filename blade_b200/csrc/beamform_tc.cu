@@ -49,8 +49,11 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <string.h>
+
 #include <mutex>
 
+#include "autotune.cuh"
 #include "common.cuh"
 #include "tc_ptx.cuh"
 
@@ -986,6 +989,13 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
                         uint32_t nf = f, ntt = tt + 1;
                         if (ntt == tpc) { ntt = 0; nf++; }
                         if (L + half + 1 < L1) direct_load(in32, g.F, g.T, nf, ntt * kM, lane, dt, half ? va : vb);
+                        if (lane < dt.nvalid && L + half + 2 < L1) {
+                            // the tile after next into L2: lanes 0-7 prefetch this thread group's rows
+                            uint32_t pf = nf, pt = ntt + 1;
+                            if (pt == tpc) { pt = 0; pf++; }
+                            prefetch_l2_bulk(in32 + ((uint64_t)(dt.a0 + lane) * g.F + pf) * g.T + pt * kM + 32u * dt.j0,
+                                             dt.nj * 128u);
+                        }
                         if (!mbar_wait(&a_empty[as + 1], aph ^ 1, abort, kWaitBudget)) {
                             record_abort(abort, 8);
                             L = L1;
@@ -1276,6 +1286,74 @@ bool tc_shape(uint64_t B, uint64_t A, TcShape& s, uint64_t T = 0, uint32_t es = 
     return true;
 }
 
+// A launch choice of the chain: mode 0 = raw ring of TMA tiles, 1 = converter
+// threads load the voltages (rate 1 CI8), with the operand ring depth, the raw
+// ring depth and the tiles per raw stage.
+struct TcChoice {
+    uint32_t mode, a_stages, r_stages, raw_tiles;
+};
+
+TcChoice tc_choice_of(const TcShape& s) {
+    return TcChoice{s.direct ? 1u : 0u, s.a_stages, s.r_stages, s.raw_tiles};
+}
+
+// Lays out shape s (image part from tc_shape) for choice c; false when c does not
+// apply to the shape or does not fit in shared memory.  Every choice computes the
+// same arithmetic in the same order within a kernel (the ring depths only change
+// scheduling), so modes 0 and 1 give bit-identical outputs.
+bool tc_apply(TcShape& s, uint64_t A, uint64_t T, uint32_t es, uint64_t rate, const TcChoice& c) {
+    const size_t op = (2ull * s.KA / 64) * 16384;
+    const size_t limit = 227 * 1024;
+    if (c.a_stages < 1 || c.a_stages > (uint32_t)kMaxStages) return false;
+    s.direct = 0;
+    s.a_stages = c.a_stages;
+    if (c.mode == 1) {
+        // direct loads run in pair mode: an even operand ring of at least four stages
+        if (es != 4 || rate != 1 || (c.a_stages & 1u) || c.a_stages < 4u) return false;
+        s.direct = 1;
+        s.raw_tiles = 1;
+        s.raw_row = kM * es;
+        s.raw_bytes = 0;
+        s.r_stages = 0;
+        s.smem = s.img_bytes + 1536 + c.a_stages * op;
+        return s.smem <= limit;
+    }
+    if (c.mode != 0 || c.r_stages < 1 || c.r_stages > (uint32_t)kMaxStages) return false;
+    if (c.raw_tiles == 2) {
+        if (es != 4 || (T / kM) % 2) return false;
+        s.raw_row = 1024;
+        s.raw_bytes = (uint32_t)A * 1024u;
+    } else if (c.raw_tiles == 1) {
+        s.raw_row = kM * es;
+        s.raw_bytes = (uint32_t)A * kM * es;
+    } else {
+        return false;
+    }
+    s.raw_tiles = c.raw_tiles;
+    s.r_stages = c.r_stages;
+    s.smem = s.img_bytes + 1536 + c.a_stages * op + c.r_stages * (size_t)s.raw_bytes;
+    return s.smem <= limit;
+}
+
+// The launch layout of a chain call: the tuned choice for this shape on this device
+// when blade_beamform_detect_tc_autotune stored one, else the heuristic default.
+bool tc_layout(uint64_t B, uint64_t A, uint64_t F, uint64_t T, uint64_t rate, uint64_t integration, uint32_t es,
+               TcShape& s, bool* tuned = nullptr, TuneEntry* entry = nullptr) {
+    if (!tc_shape(B, A, s, T, es, rate)) return false;
+    if (tuned) *tuned = false;
+    const uint64_t key[8] = {B, A, F, T, 2, rate, integration, es};
+    TuneEntry e;
+    if (tune_lookup(BLADE_TUNE_TC, key, &e)) {
+        TcShape t = s;
+        if (tc_apply(t, A, T, es, rate, TcChoice{e.params[0], e.params[1], e.params[2], e.params[3]})) {
+            s = t;
+            if (tuned) *tuned = true;
+            if (entry) *entry = e;
+        }
+    }
+    return true;
+}
+
 using TcKernel = void (*)(const TcArgs, const CUtensorMap);
 
 // Tensor map of the voltages seen as samples [A][F][T] of es bytes (CI8: one
@@ -1374,9 +1452,13 @@ namespace {
 // Launches the chain over the 64-beam chunks once the arguments are checked.
 int tc_run(const char* who, const void* in, const void* plan, void* out, uint64_t B, uint64_t A, uint64_t F,
            uint64_t T, uint64_t rate, uint64_t integration, uint32_t es, TcKernel fn, blade_stream_t stream,
-           bool pdl = false) {
+           bool pdl = false, const TcShape* force = nullptr) {
     TcShape s;
-    tc_shape(B, A, s, T, es, rate);
+    if (force) {
+        s = *force;
+    } else {
+        tc_layout(B, A, F, T, rate, integration, es, s);
+    }
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (int rc = ensure_smem(reinterpret_cast<const void*>(fn), s.smem)) return rc;
     const uint32_t U = (uint32_t)(T / (rate * integration));
@@ -1613,4 +1695,126 @@ extern "C" int blade_beamform_detect_tc_noalloc(const void* in, const void* phas
     void* plan = nullptr;
     if (int rc = noalloc_plan_address(&plan)) return rc;
     return blade_beamform_prepare_detect_tc(phasors, plan, in, out, B, A, F, T, P, rate, integration, stream);
+}
+
+// ---- autotuner ------------------------------------------------------------------
+
+namespace bb {
+namespace {
+
+// Device buffers of one tuning run, freed on every return path.
+struct DevBufs {
+    std::vector<void*> p;
+    ~DevBufs() {
+        for (void* q : p) cudaFree(q);
+    }
+    void* get(size_t bytes) {
+        void* q = nullptr;
+        if (cudaMalloc(&q, bytes < 16 ? 16 : bytes) != cudaSuccess) return nullptr;
+        p.push_back(q);
+        return q;
+    }
+};
+
+}  // namespace
+
+// Output bytes a and b (device) are identical; false on a copy failure too.
+bool tune_same(const void* a, const void* b, size_t bytes) {
+    std::vector<uint8_t> ha(bytes), hb(bytes);
+    if (cudaMemcpy(ha.data(), a, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return false;
+    if (cudaMemcpy(hb.data(), b, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return false;
+    return memcmp(ha.data(), hb.data(), bytes) == 0;
+}
+
+int tc_query(const uint64_t (&shape)[8], uint32_t* params, float* us, int* tuned) {
+    TcShape s;
+    bool t = false;
+    TuneEntry e;
+    const uint32_t es = shape[7] ? (uint32_t)shape[7] : 4u;
+    if (shape[4] != 2 || !tc_layout(shape[0], shape[1], shape[2], shape[3], shape[5], shape[6], es, s, &t, &e))
+        return set_error(BLADE_ERROR, "blade_autotune_query: unsupported tensor-core shape");
+    const TcChoice c = tc_choice_of(s);
+    for (int i = 0; i < kTuneParams; i++) params[i] = t ? e.params[i] : 0u;
+    params[0] = c.mode;
+    params[1] = c.a_stages;
+    params[2] = c.r_stages;
+    params[3] = c.raw_tiles;
+    *us = t ? e.us : 0.f;
+    *tuned = t ? 1 : 0;
+    return BLADE_SUCCESS;
+}
+
+}  // namespace bb
+
+extern "C" int blade_beamform_detect_tc_autotune(uint64_t B, uint64_t A, uint64_t F, uint64_t T, uint64_t P,
+                                                 uint64_t rate, uint64_t integration, blade_stream_t stream) {
+    using namespace bb;
+    const char* who = "blade_beamform_detect_tc_autotune";
+    if (!blade_beamform_detect_tc_supported(B, A, F, T, P, rate, integration))
+        return set_error(BLADE_ERROR, "%s: unsupported configuration", who);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const uint64_t U = T / (rate * integration);
+    const size_t in_bytes = (size_t)A * F * T * 4, ph_count = (size_t)B * A * F * 2;
+    const size_t plan_bytes = blade_beamform_tc_plan_size(B, A, F, P);
+    const size_t out_bytes = (size_t)B * F * rate * U * sizeof(float);
+    DevBufs bufs;
+    void* in = bufs.get(in_bytes);
+    void* ph = bufs.get(ph_count * sizeof(float2));
+    void* plan = bufs.get(plan_bytes);
+    void* ref = bufs.get(out_bytes);
+    void* out = bufs.get(out_bytes);
+    if (!in || !ph || !plan || !ref || !out) return set_error(BLADE_CUDA_ERROR, "%s: allocation failed", who);
+    if (int rc = tune_fill_ci8(in, in_bytes, st)) return rc;
+    if (int rc = tune_fill_phasors(ph, ph_count, st)) return rc;
+    if (int rc = blade_beamform_tc_prepare(ph, plan, B, A, F, P, stream)) return rc;
+    TcShape base;
+    tc_shape(B, A, base, T, 4, rate);
+    const TcKernel fn = pick_kernel(rate, integration);
+    // candidates: the default first, then every ring layout that fits
+    std::vector<TcChoice> cands{tc_choice_of(base)};
+    auto add = [&](TcChoice c) {
+        for (const auto& d : cands)
+            if (d.mode == c.mode && d.a_stages == c.a_stages && d.r_stages == c.r_stages && d.raw_tiles == c.raw_tiles)
+                return;
+        TcShape t = base;
+        if (tc_apply(t, A, T, 4, rate, c)) cands.push_back(c);
+    };
+    const uint32_t rings[][2] = {{8, 2}, {8, 3}, {6, 2}, {4, 4}, {4, 3}, {4, 2}, {2, 4}, {2, 2}};
+    for (uint32_t rt : {2u, 1u})
+        for (const auto& r : rings) add(TcChoice{0, r[0], r[1], rt});
+    for (uint32_t a : {8u, 6u, 4u}) add(TcChoice{1, a, 0, 1});
+    int best = -1;
+    float best_us = 0.f;
+    uint32_t ndiff = 0, ntimed = 0;
+    for (size_t i = 0; i < cands.size(); i++) {
+        TcShape t = base;
+        tc_apply(t, A, T, 4, rate, cands[i]);
+        void* dst = i == 0 ? ref : out;
+        const float us = tune_time(
+            [&]() { return tc_run(who, in, plan, dst, B, A, F, T, rate, integration, 4, fn, stream, false, &t); }, st);
+        if (us < 0.f) return set_error(BLADE_CUDA_ERROR, "%s: candidate %zu failed: %s", who, i, blade_last_error());
+        uint32_t status = 0;
+        if (int rc = blade_device_status(&status)) return rc;
+        if (status != 0) return set_error(BLADE_CUDA_ERROR, "%s: candidate %zu: device status %u", who, i, status);
+        ntimed++;
+        if (i > 0 && !tune_same(ref, out, out_bytes)) {
+            ndiff++;
+            continue;
+        }
+        if (best < 0 || us < best_us) {
+            best = (int)i;
+            best_us = us;
+        }
+    }
+    TuneEntry e = {};
+    e.params[0] = cands[best].mode;
+    e.params[1] = cands[best].a_stages;
+    e.params[2] = cands[best].r_stages;
+    e.params[3] = cands[best].raw_tiles;
+    e.params[4] = ntimed;
+    e.params[5] = ndiff;
+    e.us = best_us;
+    const uint64_t key[8] = {B, A, F, T, P, rate, integration, 4};
+    tune_store(BLADE_TUNE_TC, key, e);
+    return BLADE_SUCCESS;
 }

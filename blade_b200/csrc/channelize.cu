@@ -17,6 +17,7 @@
 // rate > 4096: a four-step FFT (C = N1 * N2): column FFTs of length N1 with the
 // inter-step twiddle, written to a workspace, then row FFTs of length N2 written
 // to the output.
+#include "autotune.cuh"
 #include "common.cuh"
 
 namespace bb {
@@ -759,6 +760,13 @@ extern "C" uint64_t blade_spectrometer_workspace_size(uint64_t A, uint64_t F, ui
     return A * F * T * P * sizeof(float2);
 }
 
+namespace bb {
+void spec_per_sm(const uint64_t (&key)[8], uint32_t (&per_sm)[2], bool* tuned = nullptr, TuneEntry* entry = nullptr);
+int spectrometer_launch(int in_type, const void* in, int out_type, void* out, void* workspace, uint64_t A, uint64_t F,
+                        uint64_t T, uint64_t integration, uint64_t out_pols, int circular,
+                        const uint32_t (&per_sm)[2], cudaStream_t s);
+}  // namespace bb
+
 extern "C" int blade_spectrometer(int in_type, const void* in, int out_type, void* out, void* workspace, uint64_t A,
                                   uint64_t F, uint64_t T, uint64_t P, uint64_t rate, uint64_t integration,
                                   uint64_t out_pols, int circular, blade_stream_t stream) {
@@ -790,13 +798,53 @@ extern "C" int blade_spectrometer(int in_type, const void* in, int out_type, voi
     if (!in || !out || !workspace) return set_error(BLADE_ERROR, "blade_spectrometer: null buffer");
     if (!aligned16(in) || !aligned16(workspace) || (reinterpret_cast<uintptr_t>(out) & 3))
         return set_error(BLADE_ERROR, "blade_spectrometer: input and workspace must be 16-byte aligned");
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t per_sm[2];
+    const uint64_t key[8] = {A, F, T, P, rate, integration, out_pols, (uint64_t)in_type};
+    spec_per_sm(key, per_sm);
+    return spectrometer_launch(in_type, in, out_type, out, workspace, A, F, T, integration, out_pols, circular,
+                               per_sm, reinterpret_cast<cudaStream_t>(stream));
+}
+
+namespace bb {
+
+// CTAs per SM of the column and row steps (both grid-stride loops): the tuned pair
+// for this shape on this device when blade_spectrometer_autotune stored one, else 2, 2.
+void spec_per_sm(const uint64_t (&key)[8], uint32_t (&per_sm)[2], bool* tuned, TuneEntry* entry) {
+    per_sm[0] = per_sm[1] = 2;
+    if (tuned) *tuned = false;
+    TuneEntry e;
+    if (tune_lookup(BLADE_TUNE_SPECTROMETER, key, &e) && e.params[0] >= 1 && e.params[0] <= 4 && e.params[1] >= 1 &&
+        e.params[1] <= 4) {
+        per_sm[0] = e.params[0];
+        per_sm[1] = e.params[1];
+        if (tuned) *tuned = true;
+        if (entry) *entry = e;
+    }
+}
+
+int spec_query(const uint64_t (&shape)[8], uint32_t* params, float* us, int* tuned) {
+    bool t = false;
+    TuneEntry e;
+    uint32_t per_sm[2];
+    spec_per_sm(shape, per_sm, &t, &e);
+    for (int i = 0; i < kTuneParams; i++) params[i] = t ? e.params[i] : 0u;
+    params[0] = per_sm[0];
+    params[1] = per_sm[1];
+    *us = t ? e.us : 0.f;
+    *tuned = t ? 1 : 0;
+    return BLADE_SUCCESS;
+}
+
+int spectrometer_launch(int in_type, const void* in, int out_type, void* out, void* workspace, uint64_t A, uint64_t F,
+                        uint64_t T, uint64_t integration, uint64_t out_pols, int circular,
+                        const uint32_t (&per_sm)[2], cudaStream_t s) {
+    const uint64_t S = T / 65536;
     float2* ws = static_cast<float2*>(workspace);
     const uint64_t batches = A * F * S;
     const size_t sm1 = (16 * 2 * kLd + 512) * sizeof(float2), sm2 = (32 * kLd + 256) * sizeof(float2);
-    const uint64_t cap = (uint64_t)sm_count() * 2;
+    const uint64_t cap1 = (uint64_t)sm_count() * per_sm[0], cap2 = (uint64_t)sm_count() * per_sm[1];
     const uint64_t g1 = batches * 16, g2 = A * F * 256;
-    const unsigned grid1 = (unsigned)(g1 < cap ? g1 : cap), grid2 = (unsigned)(g2 < cap ? g2 : cap);
+    const unsigned grid1 = (unsigned)(g1 < cap1 ? g1 : cap1), grid2 = (unsigned)(g2 < cap2 ? g2 : cap2);
     int rc;
     if (in_type == BLADE_CI8) {
         if ((rc = prepare_smem(fft256_cols_kernel<2, true>, sm1))) return rc;
@@ -822,4 +870,82 @@ extern "C" int blade_spectrometer(int in_type, const void* in, int out_type, voi
     }
 #undef BB_SPEC_ROWS
     return check_launch("blade_spectrometer");
+}
+
+}  // namespace bb
+
+extern "C" int blade_spectrometer_autotune(int in_type, int out_type, uint64_t A, uint64_t F, uint64_t T, uint64_t P,
+                                           uint64_t rate, uint64_t integration, uint64_t out_pols,
+                                           blade_stream_t stream) {
+    using namespace bb;
+    const char* who = "blade_spectrometer_autotune";
+    if (A * F == 0 || P != 2 || rate != 65536 || T % rate != 0)
+        return set_error(BLADE_ERROR, "%s: unsupported configuration", who);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const size_t n = (size_t)A * F * T * P;
+    const size_t in_bytes = n * (in_type == BLADE_CI8 ? 2 : 8);
+    const size_t ws_bytes = blade_spectrometer_workspace_size(A, F, T, P, rate);
+    const size_t out_bytes = (size_t)A * F * T / integration * out_pols * (out_type == BLADE_F16 ? 2 : 4);
+    std::vector<void*> bufs;
+    auto get = [&](size_t bytes) {
+        void* q = nullptr;
+        if (cudaMalloc(&q, bytes < 16 ? 16 : bytes) != cudaSuccess) return (void*)nullptr;
+        bufs.push_back(q);
+        return q;
+    };
+    struct Free {
+        std::vector<void*>& b;
+        ~Free() {
+            for (void* q : b) cudaFree(q);
+        }
+    } release{bufs};
+    void* in = get(in_bytes);
+    void* ws = get(ws_bytes);
+    void* ref = get(out_bytes);
+    void* out = get(out_bytes);
+    if (!in || !ws || !ref || !out) return set_error(BLADE_CUDA_ERROR, "%s: allocation failed", who);
+    if (in_type == BLADE_CI8) {
+        if (int rc = tune_fill_ci8(in, in_bytes, st)) return rc;
+    } else {
+        if (int rc = tune_fill_phasors(in, n, st)) return rc;
+    }
+    // the public entry validates the configuration
+    if (int rc = blade_spectrometer(in_type, in, out_type, ref, ws, A, F, T, P, rate, integration, out_pols, 1, stream))
+        return rc;
+    std::vector<std::pair<uint32_t, uint32_t>> cands{{2u, 2u}};
+    for (uint32_t a = 1; a <= 3; a++)
+        for (uint32_t b = 1; b <= 3; b++)
+            if (!(a == 2 && b == 2)) cands.push_back({a, b});
+    int best = -1;
+    float best_us = 0.f;
+    uint32_t ndiff = 0, ntimed = 0;
+    for (size_t i = 0; i < cands.size(); i++) {
+        const uint32_t per_sm[2] = {cands[i].first, cands[i].second};
+        void* dst = i == 0 ? ref : out;
+        const float us = tune_time(
+            [&]() {
+                return spectrometer_launch(in_type, in, out_type, dst, ws, A, F, T, integration, out_pols, 1, per_sm,
+                                           st);
+            },
+            st);
+        if (us < 0.f) return set_error(BLADE_CUDA_ERROR, "%s: candidate %zu failed: %s", who, i, blade_last_error());
+        ntimed++;
+        if (i > 0 && !tune_same(ref, out, out_bytes)) {
+            ndiff++;
+            continue;
+        }
+        if (best < 0 || us < best_us) {
+            best = (int)i;
+            best_us = us;
+        }
+    }
+    TuneEntry e = {};
+    e.params[0] = cands[best].first;
+    e.params[1] = cands[best].second;
+    e.params[4] = ntimed;
+    e.params[5] = ndiff;
+    e.us = best_us;
+    const uint64_t key[8] = {A, F, T, P, rate, integration, out_pols, (uint64_t)in_type};
+    tune_store(BLADE_TUNE_SPECTROMETER, key, e);
+    return BLADE_SUCCESS;
 }

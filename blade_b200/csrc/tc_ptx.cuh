@@ -90,6 +90,11 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int x, 
         : "memory");
 }
 
+// Asks L2 to fetch [p, p + bytes) ahead of use (p and bytes multiples of 16).
+__device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void fence_proxy_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }

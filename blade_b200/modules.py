@@ -653,6 +653,7 @@ class BeamformDetect(Module):
         number_of_output_polarizations: int = 1
         precision: str = "auto"
         block_size: int = 512
+        autotune: bool = False  # time the launch candidates of this shape at construction
 
     @dataclass
     class input:
@@ -692,6 +693,13 @@ class BeamformDetect(Module):
             # the phasor image is rebuilt every step: one per Runner slot
             n = int(lib.blade_beamform_tc_plan_size(B, A, F, P))
             self._plan = self._alloc((n,), "i8", "tensor")
+        if config.autotune:
+            from . import autotune
+
+            if prec == "fp16_split":
+                autotune.tensor_core(B, A, F, T, R, I, P=P, stream=stream)
+            else:
+                autotune.fp32(B, A, F, T, R, I, in_type=type_code(buf.dtype), P=P, stream=stream)
 
     def get_config(self):
         return self.config

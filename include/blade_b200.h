@@ -298,6 +298,57 @@ BLADE_API int blade_incoherent_detect_cf16(const void* in, const void* phasors, 
 BLADE_API int blade_device_status(uint32_t* status);
 
 /* ---------------------------------------------------------------------------
+ * Launch-shape autotuner.  The reference's only launch knob is a fixed
+ * blockSize per module (include/blade/modules/beamformer/generic.hh:20).  Here
+ * each tuning call times every launch candidate of one kernel family on the
+ * caller's shape (synthetic inputs it allocates and frees itself; CUDA events
+ * on `stream`, median of five launches after two warm-ups), checks that each
+ * candidate's output is bit-identical to the default candidate's, and stores the
+ * fastest identical one in a per-device cache keyed by family and shape.  Every
+ * later launch of that shape on that device (through any entry point of the
+ * family, eager or captured) uses the stored choice.  Tuning calls synchronise
+ * `stream` and allocate; make them at start-up, outside stream capture.
+ *
+ * Families, their shape keys (shape[0..7]) and launch choices (params[0..3]):
+ *   BLADE_TUNE_TC (blade_beamform_detect_tc, blade_beamform_prepare_detect_tc,
+ *     blade_beamform_detect_tc_noalloc): key {B, A, F, T, P, rate, integration, 4};
+ *     params {mode (0 raw ring of TMA tiles, 1 converter threads load the
+ *     voltages, 2 phasor rows in tensor memory), operand stages, raw stages,
+ *     tiles per raw stage}.
+ *   BLADE_TUNE_F32 (blade_beamform_detect_f32): key {B, A, F, T, P, rate,
+ *     integration, in_type}; params {time-group width TG (a CTA covers 4 TG
+ *     samples and 1024 / TG beams), 0, 0, 0}.
+ *   BLADE_TUNE_SPECTROMETER (blade_spectrometer): key {A, F, T, P, rate,
+ *     integration, out_pols, in_type}; params {column-step CTAs per SM, row-step
+ *     CTAs per SM, 0, 0}.
+ * params[4] = candidates timed, params[5] = candidates whose output differed from
+ * the default's (never chosen); params[6..7] = 0.
+ * ------------------------------------------------------------------------- */
+#define BLADE_TUNE_TC 1
+#define BLADE_TUNE_F32 2
+#define BLADE_TUNE_SPECTROMETER 3
+
+BLADE_API int blade_beamform_detect_tc_autotune(uint64_t B, uint64_t A, uint64_t F, uint64_t T,
+                                                uint64_t P, uint64_t rate, uint64_t integration,
+                                                blade_stream_t stream);
+BLADE_API int blade_beamform_detect_f32_autotune(int in_type, uint64_t B, uint64_t A, uint64_t F,
+                                                 uint64_t T, uint64_t P, uint64_t rate,
+                                                 uint64_t integration, blade_stream_t stream);
+BLADE_API int blade_spectrometer_autotune(int in_type, int out_type, uint64_t A, uint64_t F,
+                                          uint64_t T, uint64_t P, uint64_t rate,
+                                          uint64_t integration, uint64_t out_pols,
+                                          blade_stream_t stream);
+
+/* What a launch of `shape` in `family` uses now on the current device: params
+ * (8 values, as above) and *tuned = 1 with the measured time in *us when it comes
+ * from a tuning call, else the default choice with *tuned = 0 and *us = 0. */
+BLADE_API int blade_autotune_query(int family, const uint64_t shape[8], uint32_t params[8],
+                                   float* us, int* tuned);
+
+/* Forgets every tuned choice (all devices). */
+BLADE_API int blade_autotune_clear(void);
+
+/* ---------------------------------------------------------------------------
  * Allocation-free tensor-core chain (no counterpart in the reference).
  * Same computation, arguments and output as blade_beamform_prepare_detect_tc
  * (the split, then the chain overlapping its end), but the phasor image lives in a fixed 8 MiB

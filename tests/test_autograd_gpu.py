@@ -10,7 +10,7 @@ import pytest
 import torch
 
 from blade_b200 import synthetic as S
-from blade_b200.autograd import calibrate_phases, stokes_loss
+from blade_b200.autograd import calibrate_gains, calibrate_phases, stokes_loss
 from oracle import formulas as O
 
 pytestmark = pytest.mark.gpu
@@ -68,3 +68,21 @@ def test_phase_calibration_recovers_phases(cuda):
     err = np.degrees(np.abs(np.remainder(theta - truth + np.pi, 2 * np.pi) - np.pi))
     print(f"phase calibration: max error {err.max():.3f} deg, median {np.median(err):.3f} deg")
     assert err.max() < 1.0
+
+
+def test_gain_calibration_recovers_gains_and_phases(cuda):
+    A, F, T = 28, 192, 2048
+    rng = np.random.default_rng(S.SEEDS[5])
+    x, g = S.calibration_voltages(rng, A, F, T)
+    xt = torch.from_numpy(x.astype(np.complex64)).cuda()
+    del x
+    gains, theta = calibrate_gains(xt, steps=300, lr=0.05)
+    gains, theta = gains.cpu().numpy(), theta.cpu().numpy()
+    g_rel = np.abs(g) / np.abs(g[0])
+    gerr = np.abs(gains - g_rel) / g_rel
+    phi = np.angle(g)
+    truth = np.remainder(phi - phi[0] + np.pi, 2 * np.pi) - np.pi
+    perr = np.degrees(np.abs(np.remainder(theta - truth + np.pi, 2 * np.pi) - np.pi))
+    print(f"gain calibration: max gain ratio error {gerr.max():.4f}, max phase error {perr.max():.3f} deg")
+    assert gerr.max() < 0.02
+    assert perr.max() < 1.0

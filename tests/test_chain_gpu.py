@@ -35,6 +35,7 @@ CHAINS = [
     ("direct-ragged", 50, 40, 1152, 64, 1, 4),
     ("direct-48-beams", 64, 4, 2048, 48, 1, 16),
     ("direct-two-chunks", 64, 3, 1024, 100, 1, 8),
+    ("direct-stacked-32-beams", 64, 4, 1024, 32, 1, 2),
 ]
 
 
