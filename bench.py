@@ -779,6 +779,20 @@ def run_ours(args):
     hx, htau = make_inputs(w, SEED["dense"] + rank)
     x, tau = hx.cuda(), htau.cuda()
     ph = phasors_on_device(tau, w, stream)
+    # launch shapes tuned on this device for each timed workload (blade_*_autotune)
+    import blade_b200 as bl
+
+    tuning = {}
+    for name, wk in (("dense", w), ("ata", ATA)):
+        tc = bl.autotune.tensor_core(wk["B"], wk["A"], wk["F"], wk["T"], wk["R"], wk["I"])
+        f32 = bl.autotune.fp32(wk["B"], wk["A"], wk["F"], wk["T"], wk["R"], wk["I"])
+        tuning[name] = {"tc": {"mode": ["raw ring", "direct loads"][tc["params"][0]], "operand_stages": tc["params"][1],
+                               "raw_stages": tc["params"][2], "tiles_per_raw_stage": tc["params"][3],
+                               "candidates": tc["params"][4], "candidates_differing": tc["params"][5],
+                               "us": round(tc["us"], 1)},
+                        "fp32": {"TG": f32["params"][0], "candidates": f32["params"][4],
+                                 "candidates_differing": f32["params"][5], "us": round(f32["us"], 1)}}
+    torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         ms_tc, kern_tc, out_tc, launches = time_path(w, x, ph, "tc", args.steps, args.warmup, world)
         ms_tc_separate = time_path.separate_ms
@@ -872,6 +886,7 @@ def run_ours(args):
                          "peak_kind": f"{peak_kind} hbm_gbs (burst)",
                          "algorithmic_bytes_per_launch": algorithmic_bytes(ATA), "kernel_ms": round(akern_tc, 5),
                          "step_ms_separate_calls": round(ams_tc_separate, 5)}},
+        "tuning": tuning,
         "gpu_launches": launches * args.steps * 2 + f32_steps * 2,
         "gpu_launches_counted": "headline tc loop (split + chain per step) run twice (fused call, then separate "
                                 "calls with events), plus the fp32 loops; warm-up excluded",

@@ -72,6 +72,8 @@ _SIGNATURES = {
     "blade_spectrometer_autotune": (_int, [_int, _int, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),
     "blade_autotune_query": (_int, [_int, _u64p, C.POINTER(C.c_uint32), C.POINTER(C.c_float), C.POINTER(_int)]),
     "blade_autotune_clear": (_int, []),
+    "blade_geometric_delays": (_int, [_vp, _u64, _u64, _vp, _dbl, _dbl, _vp, _u64, _dbl, _dbl, _vp, _vp]),
+    "blade_source_direction": (_int, [_dbl, _dbl, _dbl, _dbl, C.POINTER(C.c_double)]),
 }
 
 

@@ -67,3 +67,24 @@ class Taint(enum.IntFlag):
     PRODUCER = 1 << 1
     MODIFIER = 1 << 2
     CHRONOUS = 1 << 3
+
+
+# Coordinates of the Phasor configuration (include/blade/types.hh:14-40; python
+# helpers bl.xyz / bl.lla / bl.ra_dec as the reference's bindings name them).
+from collections import namedtuple as _nt  # noqa: E402
+
+XYZ = _nt("XYZ", "x y z")
+LLA = _nt("LLA", "lon lat alt")
+RA_DEC = _nt("RA_DEC", "ra dec")
+
+
+def xyz(x, y, z):
+    return XYZ(float(x), float(y), float(z))
+
+
+def lla(lon, lat, alt):
+    return LLA(float(lon), float(lat), float(alt))
+
+
+def ra_dec(ra, dec):
+    return RA_DEC(float(ra), float(dec))

@@ -571,9 +571,16 @@ class Duplicate(Module):
 # =============================================================================
 
 class Phasor(Module):
-    """Delay -> phasor part of Modules::Phasor::ATA<CF32> (src/modules/phasor/ata.cc:176-208),
-    on the GPU in FP64.  The geometric-delay half of the reference module (ERFA
-    astrometry, ata.cc:9-173) is replaced by a delays input: [B, A] seconds."""
+    """Modules::Phasor::ATA<CF32> (src/modules/phasor/ata.cc), two input forms.
+
+    Geometric (the reference's interface): config carries the antenna positions
+    (ECEF metres), the reference antenna, the array reference position, the
+    boresight and beam coordinates (ICRS RA/Dec radians); the inputs are the
+    block's julian date and DUT1 (host F64 tensors [1]).  Each step computes the
+    geometric delays (ata.cc:9-173, blade_geometric_delays: published astrometry
+    in FP64, the A x B projections on the device), then the phasors.
+    Delays: the input is a device F64 delay_tensor [B, A] of seconds.
+    Both then compute the phasors on the GPU in FP64 (ata.cc:176-208)."""
 
     taint = Taint.CONSUMER | Taint.PRODUCER
 
@@ -589,18 +596,48 @@ class Phasor(Module):
         frequency_start_index: int = 0
         antenna_calibrations: object = None  # CF64 [A, F, 1, P] (numpy or Vector), None = unit
         block_size: int = 512
+        reference_antenna_index: int = 0
+        array_reference_position: object = None  # bl.lla(lon, lat, alt)
+        boresight_coordinate: object = None  # bl.ra_dec(ra, dec)
+        antenna_positions: object = None  # [bl.xyz(x, y, z)] * A, ECEF metres
+        beam_coordinates: object = None  # [bl.ra_dec(ra, dec)] * B
 
     @dataclass
     class input:
-        delays: object  # F64 delay_tensor [B, A] on the device
+        # geometric form: (block_julian_date, block_dut1), host F64 tensors [1];
+        # delays form: (delays,), a device F64 delay_tensor [B, A]
+        block_julian_date: object = None
+        block_dut1: object = None
+        delays: object = None
 
     def __init__(self, config, input, stream=None, it="f64", ot="cf32"):
         super().__init__()
         self.config, self._input = config, input
         c = config
-        d = as_vector(input.delays)
-        if d.dtype != "f64" or tuple(d.shape) != (c.number_of_beams, c.number_of_antennas):
-            _fail("Phasor delays must be an F64 delay_tensor [B, A].")
+        self._geometric = c.antenna_positions is not None
+        if self._geometric:
+            pos = np.asarray([tuple(p) for p in c.antenna_positions], dtype=np.float64)
+            beams = np.asarray([tuple(b) for b in c.beam_coordinates or []], dtype=np.float64)
+            if pos.ndim != 2 or pos.shape[1] != 3:
+                _fail("antenna_positions must be a list of bl.xyz.")
+            if beams.ndim != 2 or beams.shape[1] != 2 or len(beams) == 0:
+                _fail("beam_coordinates must be a non-empty list of bl.ra_dec.")
+            if c.boresight_coordinate is None:
+                _fail("boresight_coordinate is required with antenna_positions.")
+            if c.number_of_antennas != len(pos):
+                _fail(f"number_of_antennas ({c.number_of_antennas}) != {len(pos)} antenna positions.")
+            if input.block_julian_date is None or input.block_dut1 is None:
+                _fail("The geometric Phasor takes (block_julian_date, block_dut1) inputs.")
+            c.number_of_beams = len(beams)
+            self._pos = np.ascontiguousarray(pos)
+            self._beams = np.ascontiguousarray(beams)
+            lla = c.array_reference_position
+            self._lla = np.asarray(tuple(lla), dtype=np.float64) if lla is not None else None
+            self._delays = torch.empty((c.number_of_beams, c.number_of_antennas), dtype=torch.float64, device="cuda")
+        else:
+            d = as_vector(self._delays_in())
+            if d.dtype != "f64" or tuple(d.shape) != (c.number_of_beams, c.number_of_antennas):
+                _fail("Phasor delays must be an F64 delay_tensor [B, A].")
         self._cal = None
         if c.antenna_calibrations is not None:
             cal = c.antenna_calibrations
@@ -613,6 +650,11 @@ class Phasor(Module):
                        c.number_of_polarizations)
         self._output = self._alloc(self._shape, "cf32", "phasor_tensor")
 
+    def _delays_in(self):
+        # delays form: the single input (a tuple input fills the first field)
+        i = self._input
+        return i.delays if i.delays is not None else i.block_julian_date
+
     def get_config(self):
         return self.config
 
@@ -621,13 +663,30 @@ class Phasor(Module):
 
     get_output = get_phasors
 
+    def get_delays(self):
+        """Device F64 [B, A] delays of the last step (geometric form) or the input delays."""
+        return self._delays if self._geometric else as_vector(self._delays_in()).as_torch()
+
     def process(self, step=0, stream=None):
         c = self.config
-        d, out = as_vector(self._input.delays), _out(self._output)
-        _lib.call("blade_phasor_from_delays", d.data_ptr(), self._cal.data_ptr() if self._cal is not None else None,
+        s = _stream_handle(stream)
+        if self._geometric:
+            # the block's date and DUT1 are host values, read as the reference reads them
+            jd = float(as_vector(self._input.block_julian_date).as_torch().reshape(-1)[0])
+            dut1 = float(as_vector(self._input.block_dut1).as_torch().reshape(-1)[0])
+            bo = tuple(c.boresight_coordinate)
+            _lib.call("blade_geometric_delays", self._pos.ctypes.data, c.number_of_antennas,
+                      c.reference_antenna_index, self._lla.ctypes.data if self._lla is not None else None,
+                      float(bo[0]), float(bo[1]), self._beams.ctypes.data, c.number_of_beams, jd, dut1,
+                      self._delays.data_ptr(), s)
+            dptr = self._delays.data_ptr()
+        else:
+            dptr = as_vector(self._delays_in()).data_ptr()
+        out = _out(self._output)
+        _lib.call("blade_phasor_from_delays", dptr, self._cal.data_ptr() if self._cal is not None else None,
                   out.data_ptr(), c.number_of_beams, c.number_of_antennas, c.number_of_frequency_channels,
                   c.number_of_polarizations, float(c.observation_frequency_hz), float(c.channel_bandwidth_hz),
-                  float(c.total_bandwidth_hz), int(c.frequency_start_index), _stream_handle(stream))
+                  float(c.total_bandwidth_hz), int(c.frequency_start_index), s)
         return result.success
 
 

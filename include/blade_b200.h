@@ -298,6 +298,34 @@ BLADE_API int blade_incoherent_detect_cf16(const void* in, const void* phasors, 
 BLADE_API int blade_device_status(uint32_t* status);
 
 /* ---------------------------------------------------------------------------
+ * Geometric delays: the astrometric half of Modules::Phasor::ATA::process
+ * (src/modules/phasor/ata.cc:9-173; the reference calls ERFA through
+ * radiointerferometryc99, neither vendored), restated from published formulas
+ * in FP64: IAU 1982 sidereal time, IAU 1976 precession, the leading IAU 1980
+ * nutation terms and annual aberration give each source's direction s in the
+ * terrestrial frame (polar motion and refraction neglected); then
+ *   delays[b, a] = ((r_a - r_ref) . (s_b - s_boresight)) / c   [seconds]
+ * (ata.cc:39-47: TPi = (WPi - WPr) / C - (Wi - Wr) / C).
+ * antenna_positions: host F64 [A][3] earth-centred (ECEF/ITRF) metres;
+ * array_reference_lla: host F64 [3] lon, lat (rad), alt (m) or NULL (it cancels
+ * from the differences; only checked); boresight and beam_coordinates (host F64
+ * [B][2]): ICRS RA, Dec in radians; julian_date: UTC; dut1: UT1 - UTC seconds;
+ * delays: device F64 [B][A], ready for blade_phasor_from_delays.  A + B <= 1024.
+ * Parity with ERFA is unpinned (sub-arcsecond model differences).
+ * ------------------------------------------------------------------------- */
+BLADE_API int blade_geometric_delays(const double* antenna_positions, uint64_t A,
+                                     uint64_t reference_antenna, const double* array_reference_lla,
+                                     double boresight_ra, double boresight_dec,
+                                     const double* beam_coordinates, uint64_t B,
+                                     double julian_date, double dut1, double* delays,
+                                     blade_stream_t stream);
+
+/* Host only: the unit vector of (ra, dec) in the terrestrial frame at a UTC
+ * julian date (the direction blade_geometric_delays projects baselines on). */
+BLADE_API int blade_source_direction(double ra, double dec, double julian_date, double dut1,
+                                     double direction[3]);
+
+/* ---------------------------------------------------------------------------
  * Launch-shape autotuner.  The reference's only launch knob is a fixed
  * blockSize per module (include/blade/modules/beamformer/generic.hh:20).  Here
  * each tuning call times every launch candidate of one kernel family on the

@@ -312,3 +312,110 @@ def relative_l2(a: np.ndarray, ref: np.ndarray) -> float:
     ref = np.asarray(ref, dtype=a.dtype)
     den = np.linalg.norm(ref.ravel())
     return float(np.linalg.norm((a - ref).ravel()) / (den if den > 0 else 1.0))
+
+
+# --------------------------------------------------------------------------- #
+# Geometric delays (the astrometric half of Modules::Phasor::ATA)
+# --------------------------------------------------------------------------- #
+# The reference computes these with ERFA (src/modules/phasor/ata.cc:88-167) and
+# pins them only against astropy at rtol 0.5 (tests/modules/phasor/advanced.py:
+# 106-143, 183-195: w = baseline . source direction in ITRS, delay = (w_beam -
+# w_boresight) / c).  Neither ERFA nor astropy is available, so this restates the
+# published low-precision formulas the library uses (Meeus, Astronomical
+# Algorithms, 2nd ed.: eq. 12.4 sidereal time, ch. 21 IAU 1976 precession, ch. 22
+# leading IAU 1980 nutation terms, ch. 23 annual aberration); the tests pin each
+# part against Meeus' worked examples.  Parity with ERFA stays unpinned.
+
+_AS = np.pi / (180.0 * 3600.0)
+_DEG = np.pi / 180.0
+C_LIGHT = 299792458.0
+
+
+def _r1(t):
+    c, s = np.cos(t), np.sin(t)
+    return np.array([[1, 0, 0], [0, c, s], [0, -s, c]])
+
+
+def _r2(t):
+    c, s = np.cos(t), np.sin(t)
+    return np.array([[c, 0, -s], [0, 1, 0], [s, 0, c]])
+
+
+def _r3(t):
+    c, s = np.cos(t), np.sin(t)
+    return np.array([[c, s, 0], [-s, c, 0], [0, 0, 1]])
+
+
+def gmst_deg(jd_ut1: float) -> float:
+    """Greenwich mean sidereal time in degrees (Meeus eq. 12.4, IAU 1982)."""
+    du = jd_ut1 - 2451545.0
+    tu = du / 36525.0
+    return (280.46061837 + 360.98564736629 * du + 0.000387933 * tu * tu - tu ** 3 / 38710000.0) % 360.0
+
+
+def nutation(t: float):
+    """(dpsi, deps, eps0) in radians for Julian centuries t of TT from J2000.0:
+    the four leading IAU 1980 terms (Meeus ch. 22, 0.5" / 0.1")."""
+    om = (125.04452 - 1934.136261 * t) * _DEG
+    ls = (280.4665 + 36000.7698 * t) * _DEG
+    lm = (218.3165 + 481267.8813 * t) * _DEG
+    dpsi = (-17.20 * np.sin(om) - 1.32 * np.sin(2 * ls) - 0.23 * np.sin(2 * lm) + 0.21 * np.sin(2 * om)) * _AS
+    deps = (9.20 * np.cos(om) + 0.57 * np.cos(2 * ls) + 0.10 * np.cos(2 * lm) - 0.09 * np.cos(2 * om)) * _AS
+    eps0 = (84381.448 - 46.8150 * t - 0.00059 * t * t + 0.001813 * t ** 3) * _AS
+    return dpsi, deps, eps0
+
+
+def precession_matrix(t: float) -> np.ndarray:
+    """IAU 1976 precession from J2000.0 to t Julian centuries (Meeus eq. 21.3)."""
+    zeta = (2306.2181 * t + 0.30188 * t * t + 0.017998 * t ** 3) * _AS
+    z = (2306.2181 * t + 1.09468 * t * t + 0.018203 * t ** 3) * _AS
+    theta = (2004.3109 * t - 0.42665 * t * t - 0.041833 * t ** 3) * _AS
+    return _r3(-z) @ _r2(theta) @ _r3(-zeta)
+
+
+def source_itrs(ra: float, dec: float, jd_utc: float, dut1: float) -> np.ndarray:
+    """Unit vector of ICRS (ra, dec) in the terrestrial frame (polar motion
+    neglected): R3(GAST) N P applied to the annually aberrated direction."""
+    t = (jd_utc + 69.184 / 86400.0 - 2451545.0) / 36525.0
+    dpsi, deps, eps0 = nutation(t)
+    eps = eps0 + deps
+    l0 = (280.46646 + 36000.76983 * t + 0.0003032 * t * t) * _DEG
+    ma = (357.52911 + 35999.05029 * t - 0.0001537 * t * t) * _DEG
+    cen = ((1.914602 - 0.004817 * t - 0.000014 * t * t) * np.sin(ma) + (0.019993 - 0.000101 * t) * np.sin(2 * ma)
+           + 0.000289 * np.sin(3 * ma)) * _DEG
+    lsun = l0 + cen
+    kappa = 20.49552 * _AS
+    p = np.array([np.cos(dec) * np.cos(ra), np.cos(dec) * np.sin(ra), np.sin(dec)])
+    p = p + kappa * np.array([np.sin(lsun), -np.cos(lsun) * np.cos(eps), -np.cos(lsun) * np.sin(eps)])
+    p = p / np.linalg.norm(p)
+    gast = gmst_deg(jd_utc + dut1 / 86400.0) * _DEG + dpsi * np.cos(eps)
+    n = _r1(-eps) @ _r3(-dpsi) @ _r1(eps0)
+    return _r3(gast) @ n @ precession_matrix(t) @ p
+
+
+def geometric_delays(positions, reference: int, boresight, beams, jd_utc: float, dut1: float) -> np.ndarray:
+    """delays[b, a] = ((r_a - r_ref) . (s_b - s_boresight)) / c (ata.cc:39-47)."""
+    r = np.asarray(positions, dtype=np.float64)
+    bl = r - r[reference]
+    s0 = source_itrs(boresight[0], boresight[1], jd_utc, dut1)
+    out = np.empty((len(beams), len(r)))
+    for b, (ra, dec) in enumerate(beams):
+        out[b] = bl @ (source_itrs(ra, dec, jd_utc, dut1) - s0) / C_LIGHT
+    return out
+
+
+def delays_via_hour_angle(positions, reference: int, lon: float, boresight, beams, jd_utc: float, dut1: float):
+    """The same delays by the reference's route (ata.cc:17-47): array-centred XYZ
+    (ECEF rotated by the reference longitude), W of the UVW frame of each source's
+    apparent hour angle and declination (Thompson, Moran & Swenson eq. 4.1)."""
+    r = np.asarray(positions, dtype=np.float64) - np.asarray(positions, dtype=np.float64)[reference]
+    xyz = r @ _r3(lon).T  # X toward the local meridian, Y east, Z north
+
+    def w_of(ra, dec):
+        s = source_itrs(ra, dec, jd_utc, dut1)
+        ha = lon - np.arctan2(s[1], s[0])  # local apparent hour angle
+        d = np.arcsin(s[2])
+        return np.cos(d) * np.cos(ha) * xyz[:, 0] - np.cos(d) * np.sin(ha) * xyz[:, 1] + np.sin(d) * xyz[:, 2]
+
+    w0 = w_of(*boresight)
+    return np.stack([(w_of(ra, dec) - w0) / C_LIGHT for ra, dec in beams])
