@@ -333,6 +333,183 @@ __device__ __forceinline__ void dft16(float2 (&v)[16]) {
     for (int k = 0; k < 16; k++) v[k] = t[k];
 }
 
+// ---- rates 2, 4, 8, 16: one spectrum per thread in registers ----------------
+// The shared-memory Stockham above pays a load / sync / pass / sync / store round per
+// group; a transform this short fits a thread's registers instead.  Thread = one
+// spectrum s of one (a, f): R consecutive samples (P = 2: both polarisations in one
+// 16-byte word) in, the R fftshifted bins out, bin k of every spectrum of the row
+// block written side by side (consecutive threads, consecutive 16-byte stores).
+template <int R>
+__device__ __forceinline__ void dft_small(float2 (&v)[R]) {
+    if constexpr (R == 2) {
+        const float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (R == 4) {
+        dft4(v[0], v[1], v[2], v[3]);  // outputs in natural order
+    } else if constexpr (R == 8) {
+        // radix 2 x 4: X[k] = E[k mod 4] + w8^k O[k mod 4], E / O = DFT-4 of the even / odd samples
+        float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6], o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+        dft4(e0, e1, e2, e3);
+        dft4(o0, o1, o2, o3);
+        const float h = 0.70710678118654752f;
+        const float2 t0 = o0, t1 = make_float2(h * (o1.x + o1.y), h * (o1.y - o1.x)), t2 = mul_mi(o2),
+                     t3 = make_float2(h * (o3.y - o3.x), -h * (o3.x + o3.y));
+        v[0] = cadd(e0, t0);
+        v[4] = csub(e0, t0);
+        v[1] = cadd(e1, t1);
+        v[5] = csub(e1, t1);
+        v[2] = cadd(e2, t2);
+        v[6] = csub(e2, t2);
+        v[3] = cadd(e3, t3);
+        v[7] = csub(e3, t3);
+    } else {
+        static_assert(R == 16, "rates 2, 4, 8, 16");
+        dft16(v);
+    }
+}
+
+template <int R, int P>
+__global__ void __launch_bounds__(256) fft_reg_kernel(const float2* __restrict__ in, float2* __restrict__ out,
+                                                      uint64_t rows, uint32_t S) {
+    const uint64_t n = rows * S;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t af = i / S;
+        const uint32_t sp = (uint32_t)(i - af * S);
+        const float2* src = in + i * R * P;  // spectrum sp of row af starts at sample (af S + sp) R
+        float2 x[P][R];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            if constexpr (P == 2) {
+                const float4 v = __ldg(reinterpret_cast<const float4*>(src) + r);
+                x[0][r] = make_float2(v.x, v.y);
+                x[1][r] = make_float2(v.z, v.w);
+            } else {
+                x[0][r] = __ldg(src + r);
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < P; p++) dft_small<R>(x[p]);
+        // out[a, f R + k, s, p] = X[(k + R / 2) mod R]
+        float2* dst = out + ((af * R) * S + sp) * P;
+#pragma unroll
+        for (int k = 0; k < R; k++) {
+            const int kk = (k + R / 2) % R;
+            if constexpr (P == 2) {
+                stg_f4(dst + (uint64_t)k * S * 2, make_float4(x[0][kk].x, x[0][kk].y, x[1][kk].x, x[1][kk].y));
+            } else {
+                dst[(uint64_t)k * S] = x[0][kk];
+            }
+        }
+    }
+}
+
+// ---- rate 8192: one transform per CTA unit, no workspace ---------------------
+// N = 8192 = 16 x 16 x 32, n = t + 512 m, t = 32 u + v, k = k1 + 16 k2a + 256 k2b:
+//   Y[k1][t]      = w8192^(t k1)  DFT16_m(x[t + 512 m])[k1]
+//   Z[k1][k2a][v] = w512^(v k2a)  DFT16_u(Y[k1][32 u + v])[k2a]
+//   X[k]          = DFT32_v(Z[k1][k2a][v])[k2b]
+// A unit is one polarisation of one spectrum (a, f, s); 256 threads, the 8192
+// values in shared memory between the three register stages (Y and Z share one
+// buffer, rows padded to 529 and 33 so that every access of a half-warp is one
+// wavefront).  Twiddle powers come from one sincospif and a recurrence of 15
+// complex products (a few FP32 ulps).  The output bins of a unit are its own
+// (written after all of its inputs are read), so rate == T runs in place.
+constexpr uint32_t kN8 = 8192, kZ1 = 529, kZ2 = 33;
+
+// w32^k = exp(-2 pi i k / 32), k < 16
+__device__ __constant__ float2 c_w32[16] = {
+    {1.000000000e+00f, -0.000000000e+00f}, {9.807852804e-01f, -1.950903220e-01f},
+    {9.238795325e-01f, -3.826834324e-01f}, {8.314696123e-01f, -5.555702330e-01f},
+    {7.071067812e-01f, -7.071067812e-01f}, {5.555702330e-01f, -8.314696123e-01f},
+    {3.826834324e-01f, -9.238795325e-01f}, {1.950903220e-01f, -9.807852804e-01f},
+    {0.000000000e+00f, -1.000000000e+00f}, {-1.950903220e-01f, -9.807852804e-01f},
+    {-3.826834324e-01f, -9.238795325e-01f}, {-5.555702330e-01f, -8.314696123e-01f},
+    {-7.071067812e-01f, -7.071067812e-01f}, {-8.314696123e-01f, -5.555702330e-01f},
+    {-9.238795325e-01f, -3.826834324e-01f}, {-9.807852804e-01f, -1.950903220e-01f}};
+
+template <int P>
+__global__ void __launch_bounds__(256, 2) fft8192_kernel(const float2* __restrict__ in, float2* __restrict__ out,
+                                                          uint64_t units, uint32_t S) {
+    extern __shared__ __align__(16) float2 sm[];  // 16 rows of kZ1
+    const uint32_t tid = threadIdx.x;
+    for (uint64_t unit = blockIdx.x; unit < units; unit += gridDim.x) {
+        const uint32_t p = (uint32_t)(unit % P);
+        const uint64_t as = unit / P;  // (a, f) row x S + s
+        const uint64_t af = as / S;
+        const uint32_t s = (uint32_t)(as - af * S);
+        const float2* src = in + as * (uint64_t)kN8 * P + p;  // sample n at src[n P]
+        // stage A: columns t = tid, tid + 256
+#pragma unroll 1
+        for (uint32_t c = 0; c < 2; c++) {
+            const uint32_t t = tid + 256 * c;
+            float2 v[16];
+#pragma unroll
+            for (int m = 0; m < 16; m++) v[m] = src[(uint64_t)(t + 512 * m) * P];
+            dft16(v);
+            float2 w1, wk = make_float2(1.f, 0.f);
+            sincospif(-2.f * (float)t / 8192.f, &w1.y, &w1.x);
+#pragma unroll
+            for (int k1 = 0; k1 < 16; k1++) {
+                if (k1) {
+                    wk = cmul(wk, w1);
+                    v[k1] = cmul(v[k1], wk);
+                }
+                sm[k1 * kZ1 + t] = v[k1];
+            }
+        }
+        __syncthreads();
+        // stage B: pairs q = tid, tid + 256 -> (k1, v) = (q / 32, q % 32); all reads first
+        float2 y[2][16];
+#pragma unroll
+        for (uint32_t c = 0; c < 2; c++) {
+            const uint32_t q = tid + 256 * c, k1 = q >> 5, vv = q & 31;
+#pragma unroll
+            for (int u = 0; u < 16; u++) y[c][u] = sm[k1 * kZ1 + 32 * u + vv];
+        }
+        __syncthreads();
+#pragma unroll
+        for (uint32_t c = 0; c < 2; c++) {
+            const uint32_t q = tid + 256 * c, k1 = q >> 5, vv = q & 31;
+            dft16(y[c]);
+            float2 w1, wk = make_float2(1.f, 0.f);
+            sincospif(-2.f * (float)vv / 512.f, &w1.y, &w1.x);
+#pragma unroll
+            for (int k2a = 0; k2a < 16; k2a++) {
+                if (k2a) {
+                    wk = cmul(wk, w1);
+                    y[c][k2a] = cmul(y[c][k2a], wk);
+                }
+                sm[k1 * kZ1 + k2a * kZ2 + vv] = y[c][k2a];
+            }
+        }
+        __syncthreads();
+        // stage C: thread (k1, k2a) = (tid % 16, tid / 16), a 32-point DFT over v as
+        // two 16-point DFTs of the even and odd samples
+        {
+            const uint32_t k1 = tid & 15, k2a = tid >> 4;
+            float2 e[16], o[16];
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                e[i] = sm[k1 * kZ1 + k2a * kZ2 + 2 * i];
+                o[i] = sm[k1 * kZ1 + k2a * kZ2 + 2 * i + 1];
+            }
+            dft16(e);
+            dft16(o);
+            // out[a, f N + kout, s, p], kout = (k + N / 2) mod N (fftshift)
+            float2* dst = out + ((af * kN8) * S + s) * P + p;
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                const float2 t = cmul(o[k], c_w32[k]);
+                const uint32_t k0 = k1 + 16 * k2a + 256 * k, k16 = k0 + 4096;  // X[k0] and X[k0 + 4096]
+                dst[(uint64_t)((k0 + 4096) & 8191) * S * P] = cadd(e[k], t);
+                dst[(uint64_t)((k16 + 4096) & 8191) * S * P] = csub(e[k], t);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // Column step for N = 65536 (N1 = N2 = 256): one CTA = one (a, f, s) spectrum, 16
 // consecutive columns j2, both polarisations (32 FFTs x 16 threads = 512 threads).
 // Output ws[((batch P + p) 256 + k1) 256 + j2] = w65536^(j2 k1) FFT256_j1(x[256 j1 + j2])[k1].
@@ -642,7 +819,7 @@ bool split_large(uint64_t N, uint64_t& N1, uint64_t& N2) {
 }  // namespace bb
 
 extern "C" uint64_t blade_channelize_workspace_size(uint64_t A, uint64_t F, uint64_t T, uint64_t P, uint64_t rate) {
-    if (rate <= bb::kSmallMax) return 0;
+    if (rate <= bb::kSmallMax || rate == bb::kN8) return 0;
     return A * F * T * P * sizeof(float2);
 }
 
@@ -672,6 +849,21 @@ extern "C" int blade_channelize(const void* in, void* out, void* workspace, uint
     float2* dst = static_cast<float2*>(out);
     const uint64_t S = T / rate;
     const int blocks_per_sm = 2;
+    if ((rate == 2 || rate == 4 || rate == 8 || rate == 16) && S < (1ull << 32)) {
+        const uint64_t rows = A * F;
+        const unsigned grid = grid_for(rows * S, 256);
+#define BB_FFT_REG(RR)                                                                               \
+    do {                                                                                             \
+        if (P == 2) fft_reg_kernel<RR, 2><<<grid, 256, 0, s>>>(src, dst, rows, (uint32_t)S);         \
+        else fft_reg_kernel<RR, 1><<<grid, 256, 0, s>>>(src, dst, rows, (uint32_t)S);                \
+    } while (0)
+        if (rate == 2) BB_FFT_REG(2);
+        else if (rate == 4) BB_FFT_REG(4);
+        else if (rate == 8) BB_FFT_REG(8);
+        else BB_FFT_REG(16);
+#undef BB_FFT_REG
+        return check_launch("blade_channelize");
+    }
     if (rate <= kSmallMax) {
         Plan plan;
         if (!make_plan(rate, plan))
@@ -694,6 +886,21 @@ extern "C" int blade_channelize(const void* in, void* out, void* workspace, uint
             fft_small_kernel<1><<<grid, kThreads, smem, s>>>(src, dst, (uint32_t)A, (uint32_t)F, (uint32_t)T,
                                                             (uint32_t)rate, (uint32_t)SB, plan);
         }
+        return check_launch("blade_channelize");
+    }
+    if (rate == kN8) {
+        const uint64_t units = A * F * S * P;
+        const size_t smem = 16 * kZ1 * sizeof(float2);
+        int rc;
+        if (P == 2) {
+            if ((rc = prepare_smem(fft8192_kernel<2>, smem))) return rc;
+        } else {
+            if ((rc = prepare_smem(fft8192_kernel<1>, smem))) return rc;
+        }
+        const uint64_t cap = (uint64_t)sm_count() * 2;
+        const unsigned grid = (unsigned)(units < cap ? units : cap);
+        if (P == 2) fft8192_kernel<2><<<grid, 256, smem, s>>>(src, dst, units, (uint32_t)S);
+        else fft8192_kernel<1><<<grid, 256, smem, s>>>(src, dst, units, (uint32_t)S);
         return check_launch("blade_channelize");
     }
     if (!workspace) return set_error(BLADE_ERROR, "blade_channelize: rate %llu needs a workspace of %llu bytes",

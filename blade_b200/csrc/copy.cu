@@ -192,6 +192,39 @@ extern "C" int blade_permute(uint64_t elem_bytes, const void* in, void* out, con
     if (in == out) return set_error(BLADE_ERROR, "blade_permute: in-place permutation is not supported");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
 
+    // Input axes that stay adjacent and in order in the output move as one axis:
+    // merge them first (e.g. AFTP -> ATPF is [A][F][T P] -> [A][T P][F], a batched
+    // transpose of full-width tiles instead of tiles two elements wide), then pad
+    // the merged rank back to four with leading axes of extent 1.
+    uint64_t mshape[4] = {1, 1, 1, 1}, midx[4] = {0, 1, 2, 3};
+    {
+        int first[4], last[4], ng = 0;  // groups of input axes in output order
+        for (int i = 0; i < 4; i++) {
+            if (ng > 0 && indexes[i] == (uint64_t)last[ng - 1] + 1) {
+                last[ng - 1] = (int)indexes[i];
+            } else {
+                first[ng] = last[ng] = (int)indexes[i];
+                ng++;
+            }
+        }
+        int rank[4];  // each group's position among the groups in input order
+        for (int g = 0; g < ng; g++) {
+            rank[g] = 0;
+            for (int h = 0; h < ng; h++)
+                if (first[h] < first[g]) rank[g]++;
+        }
+        const int pad = 4 - ng;
+        for (int g = 0; g < ng; g++) {
+            uint64_t ext = 1;
+            for (int d = first[g]; d <= last[g]; d++) ext *= shape[d];
+            mshape[pad + rank[g]] = ext;
+            midx[pad + g] = (uint64_t)(pad + rank[g]);
+        }
+        for (int i = 0; i < pad; i++) midx[i] = (uint64_t)i;
+        shape = mshape;
+        indexes = midx;
+    }
+
     // Input strides and output strides expressed per input axis.
     uint64_t is[4], os_out[4], os_in[4], oshape[4];
     is[3] = 1;

@@ -128,6 +128,14 @@ CH_CASES = [
     (1, 2, 16384, 2, 8192),     # four-step path
     (1, 2, 131072, 2, 65536),   # the spectrometer NFFT
     (3, 4, 20, 2, 2),
+    # rates 2, 4, 8, 16 run one spectrum per thread in registers: both pol counts
+    (3, 5, 96, 1, 4),
+    (2, 3, 256, 2, 8),
+    (2, 3, 256, 1, 8),
+    (2, 3, 512, 2, 16),
+    (2, 3, 512, 1, 16),
+    (2, 2, 64, 1, 2),
+    (2, 3, 24576, 1, 8192),     # rate 8192: one transform per CTA unit, three spectra per row
 ]
 
 
@@ -143,9 +151,10 @@ def test_channelizer(cuda, A, F, T, P, rate):
     assert rel_l2(host(yd), O.channelize(x, rate)) < TOL
 
 
-def test_channelizer_in_place_rate_equals_T(cuda):
-    rng = np.random.default_rng(77)
-    A, F, T, P = 3, 7, 256, 2
+@pytest.mark.parametrize("A,F,T,P", [(3, 7, 256, 2), (3, 5, 8192, 2), (2, 3, 8192, 1), (2, 2, 4, 2)])
+def test_channelizer_in_place_rate_equals_T(cuda, A, F, T, P):
+    # rate == T in place, as the reference module runs it (its benchmark: rate 8192)
+    rng = np.random.default_rng(77 + T + P)
     x = crand(rng, (A, F, T, P))
     xd = c64(x)
     call("blade_channelize", ptr(xd), ptr(xd), None, A, F, T, P, T, stream())
