@@ -2,7 +2,8 @@
 
     python profile_case.py --workload ata-production --path tc --launches 4
 
-Workloads: ata-small (A=20 F=96 T=256 B=8 rate 1 I=4), ata-production
+Workloads: channelizer-rate4 and channelizer-rate8192 (the Channelizer module on
+CF32 [16, 192, 8192, 2], path channelize), ata-small (A=20 F=96 T=256 B=8 rate 1 I=4), ata-production
 (A=28 F=192 T=8192 B=16 rate 4 I=4), dense-64x64 (A=64 F=256 T=8192 B=64 rate 1
 I=8), spectrometer (A=1 F=64 T=2^20, rate 65536, I=8, no beamformer) and
 spectrometer-small (the same with F=16, for full profiler captures), calibration
@@ -33,13 +34,16 @@ WORKLOADS = {
     "spectrometer-small": dict(A=1, F=16, T=1 << 20, B=0, R=65536, I=8),
     "calibration": dict(A=28, F=192, T=2048, B=1, R=1, I=1),
     "modeb": dict(A=28, F=192, T=8192, B=16, R=4, I=4),
+    # the standalone Channelizer module on CF32 [16, 192, 8192, 2] (path channelize)
+    "channelizer-rate4": dict(A=16, F=192, T=8192, B=0, R=4, I=1),
+    "channelizer-rate8192": dict(A=16, F=192, T=8192, B=0, R=8192, I=1),
 }
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="ata-production", choices=sorted(WORKLOADS))
-    ap.add_argument("--path", default="tc", choices=["tc", "f32", "modules", "adjoint", "fused"])
+    ap.add_argument("--path", default="tc", choices=["tc", "f32", "modules", "adjoint", "fused", "channelize"])
     ap.add_argument("--launches", type=int, default=4)
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
@@ -64,6 +68,16 @@ def main():
                       P, I, s)
         torch.cuda.synchronize()
         print(f"modeb tc: {args.launches} launches ok")
+        return
+    if args.path == "channelize":
+        xc = torch.randn((A, F, T, P, 2), generator=g, device="cuda").view(torch.complex64).reshape(A, F, T, P)
+        yc = torch.empty_like(xc)
+        wsb = int(lib.blade_channelize_workspace_size(A, F, T, P, R))
+        ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
+        for _ in range(args.launches):
+            _lib.call("blade_channelize", xc.data_ptr(), yc.data_ptr(), ws.data_ptr() if wsb else None, A, F, T, P, R, s)
+        torch.cuda.synchronize()
+        print(f"{args.workload} channelize: {args.launches} launches ok")
         return
     if args.path == "adjoint":
         xc = torch.complex(torch.randn((A, F, T, P), generator=g, device="cuda"),
