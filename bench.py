@@ -593,34 +593,45 @@ def adjoint_step(steps, warmup):
     from blade_b200 import _lib
 
     _lib.load()
-    A, F, T, P, B = (ADJ[k] for k in ("A", "F", "T", "P", "B"))
+    A, F, T, P = (ADJ[k] for k in ("A", "F", "T", "P"))
     s = torch.cuda.current_stream()
     sh = s.cuda_stream
     g = torch.Generator(device="cuda").manual_seed(1005)
     x = torch.complex(torch.randn((A, F, T, P), generator=g, device="cuda"),
                       torch.randn((A, F, T, P), generator=g, device="cuda"))
-    ph = torch.polar(torch.ones((B, A, F, 1, P), device="cuda"),
-                     torch.rand((B, A, F, 1, P), generator=g, device="cuda") * 6.283185307)
-    grad = torch.empty_like(ph)
-    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
-    for _ in range(warmup):
-        _lib.call("blade_beamform_detect_adjoint", x.data_ptr(), ph.data_ptr(), grad.data_ptr(), loss.data_ptr(),
-                  B, A, F, T, P, sh)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(s)
-    for _ in range(steps):
-        _lib.call("blade_beamform_detect_adjoint", x.data_ptr(), ph.data_ptr(), grad.data_ptr(), loss.data_ptr(),
-                  B, A, F, T, P, sh)
-    e1.record(s)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    nbytes = A * F * T * P * 8 + 2 * B * A * F * P * 8
     hbm = load_peaks()[0]
-    return {"workload": "A=28 B=1 F=192 T=2048 P=2 CF32, Stokes loss + dL/dconj(w)",
-            "ms_per_step": round(ms, 4), "gbs": round(nbytes / (ms * 1e-3) / 1e9, 1),
-            "frac_of_hbm": round(nbytes / (ms * 1e-3) / 1e9 / hbm, 3),
-            "macs_fwd_plus_adj": 2 * 4 * B * A * F * T * P}
+
+    def timed(entry, B):
+        ph = torch.polar(torch.ones((B, A, F, 1, P), device="cuda"),
+                         torch.rand((B, A, F, 1, P), generator=g, device="cuda") * 6.283185307)
+        grad = torch.empty_like(ph)
+        loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+
+        def call():
+            _lib.call(entry, x.data_ptr(), ph.data_ptr(), grad.data_ptr(), loss.data_ptr(), B, A, F, T, P, sh)
+
+        for _ in range(warmup):
+            call()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(steps):
+            call()
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        nbytes = A * F * T * P * 8 + 2 * B * A * F * P * 8
+        return {"ms_per_step": round(ms, 4), "gbs": round(nbytes / (ms * 1e-3) / 1e9, 1),
+                "frac_of_hbm": round(nbytes / (ms * 1e-3) / 1e9 / hbm, 3),
+                "macs_fwd_plus_adj": 2 * 4 * B * A * F * T * P}
+
+    res = {"workload": "A=28 F=192 T=2048 P=2 CF32, Stokes loss + dL/dconj(w); B=1 (the calibration block) and B=16"}
+    res.update(timed("blade_beamform_detect_adjoint", 1))  # the default dispatch at B = 1: CUDA cores
+    res["b1_tensor_cores"] = timed("blade_beamform_detect_adjoint_tc", 1)
+    res["b16_tensor_cores"] = timed("blade_beamform_detect_adjoint_tc", 16)
+    res["b16_cuda_cores"] = timed("blade_beamform_detect_adjoint_f32", 16)
+    res["b16_speedup_tensor_cores"] = round(res["b16_cuda_cores"]["ms_per_step"] / res["b16_tensor_cores"]["ms_per_step"], 2)
+    return res
 
 
 GATHER_SHAPES = [("ata", (5, 192, 8192, 2)), ("vla", (5, 131072, 1, 2))]

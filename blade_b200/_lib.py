@@ -65,6 +65,8 @@ _SIGNATURES = {
     "blade_prechannelize_cf16": (_int, [_vp, _vp, _u64, _u64, _u64, _u64, _u64, _int, _vp]),
     "blade_incoherent_detect_cf16": (_int, [_vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp]),
     "blade_beamform_detect_adjoint": (_int, [_vp, _vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp]),
+    "blade_beamform_detect_adjoint_f32": (_int, [_vp, _vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp]),
+    "blade_beamform_detect_adjoint_tc": (_int, [_vp, _vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp]),
     "blade_device_status": (_int, [C.POINTER(C.c_uint32)]),
     "blade_beamform_detect_tc_noalloc": (_int, [_vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),
     "blade_beamform_detect_tc_autotune": (_int, [_u64, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),

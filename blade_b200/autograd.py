@@ -24,7 +24,11 @@ import torch
 from . import _lib
 
 
-def _adjoint(x: torch.Tensor, w: torch.Tensor):
+_ENTRY = {"auto": "blade_beamform_detect_adjoint", "tensor_cores": "blade_beamform_detect_adjoint_tc",
+          "fp32": "blade_beamform_detect_adjoint_f32"}
+
+
+def _adjoint(x: torch.Tensor, w: torch.Tensor, path: str = "auto"):
     if not (x.is_cuda and w.is_cuda):
         raise RuntimeError("stokes_loss needs CUDA tensors")
     if x.dtype != torch.complex64 or w.dtype != torch.complex64:
@@ -37,8 +41,10 @@ def _adjoint(x: torch.Tensor, w: torch.Tensor):
         raise RuntimeError(f"weights shape {tuple(w.shape)} does not match voltages {tuple(x.shape)}")
     grad = torch.empty_like(w)
     loss = torch.empty(1, dtype=torch.float64, device=x.device)
-    _lib.call("blade_beamform_detect_adjoint", x.data_ptr(), w.data_ptr(), grad.data_ptr(), loss.data_ptr(), B, A, F,
-              T, P, torch.cuda.current_stream().cuda_stream)
+    if path not in _ENTRY:
+        raise ValueError(f"path must be one of {sorted(_ENTRY)}")
+    _lib.call(_ENTRY[path], x.data_ptr(), w.data_ptr(), grad.data_ptr(), loss.data_ptr(), B, A, F, T, P,
+              torch.cuda.current_stream().cuda_stream)
     return loss[0], grad
 
 
@@ -46,8 +52,8 @@ class StokesLoss(torch.autograd.Function):
     """L(w) = -sum Stokes-I(beamform(x, w)); gradient w.r.t. the complex weights."""
 
     @staticmethod
-    def forward(ctx, x: torch.Tensor, w: torch.Tensor):
-        loss, g = _adjoint(x.detach(), w.detach())
+    def forward(ctx, x: torch.Tensor, w: torch.Tensor, path: str = "auto"):
+        loss, g = _adjoint(x.detach(), w.detach(), path)
         ctx.save_for_backward(g)
         return loss
 
@@ -55,14 +61,16 @@ class StokesLoss(torch.autograd.Function):
     def backward(ctx, grad_out):
         (g,) = ctx.saved_tensors
         # g = dL/d conj(w); torch wants dL/dRe w + i dL/dIm w = 2 g (L is real).
-        return None, (2.0 * grad_out.to(torch.float32)) * g
+        return None, (2.0 * grad_out.to(torch.float32)) * g, None
 
 
-def stokes_loss(x: torch.Tensor, w: torch.Tensor) -> torch.Tensor:
-    return StokesLoss.apply(x, w)
+def stokes_loss(x: torch.Tensor, w: torch.Tensor, path: str = "auto") -> torch.Tensor:
+    """path: "auto" (tensor cores from 8 beams up where the shape allows, else CUDA
+    cores), "tensor_cores" (blade_beamform_detect_adjoint_tc) or "fp32"."""
+    return StokesLoss.apply(x, w, path)
 
 
-def calibrate_phases(x: torch.Tensor, steps: int = 200, lr: float = 0.05, ref: int = 0):
+def calibrate_phases(x: torch.Tensor, steps: int = 200, lr: float = 0.05, ref: int = 0, path: str = "auto"):
     """Per-antenna phase calibration of a boresight beam by gradient ascent on its
     summed Stokes-I: w[0, a, f, 0, p] = exp(-i theta_a) / sqrt(A), maximise
     sum |y|^2 over theta (Adam).  Returns theta relative to antenna ``ref``,
@@ -76,7 +84,7 @@ def calibrate_phases(x: torch.Tensor, steps: int = 200, lr: float = 0.05, ref: i
         opt.zero_grad()
         w = torch.exp(-1j * theta.to(torch.complex64)) / math.sqrt(A)
         w = w.view(1, A, 1, 1, 1).expand(1, A, F, 1, P).contiguous()
-        loss = stokes_loss(x, w) * scale  # minimising -S maximises S
+        loss = stokes_loss(x, w, path) * scale  # minimising -S maximises S
         loss.backward()
         opt.step()
     with torch.no_grad():
@@ -84,7 +92,7 @@ def calibrate_phases(x: torch.Tensor, steps: int = 200, lr: float = 0.05, ref: i
         return torch.remainder(rel + math.pi, 2 * math.pi) - math.pi
 
 
-def calibrate_gains(x: torch.Tensor, steps: int = 300, lr: float = 0.05, ref: int = 0):
+def calibrate_gains(x: torch.Tensor, steps: int = 300, lr: float = 0.05, ref: int = 0, path: str = "auto"):
     """Per-antenna gain and phase calibration of a boresight beam by gradient ascent
     on its summed Stokes-I over complex weights of unit norm, w = u / |u| with
     w[0, a, f, 0, p] = w_a (Adam on u).  For voltages v_a = g_a exp(i phi_a) s + n_a
@@ -101,7 +109,7 @@ def calibrate_gains(x: torch.Tensor, steps: int = 300, lr: float = 0.05, ref: in
         opt.zero_grad()
         wa = u / torch.linalg.vector_norm(u)
         w = wa.view(1, A, 1, 1, 1).expand(1, A, F, 1, P).contiguous()
-        loss = stokes_loss(x, w) * scale
+        loss = stokes_loss(x, w, path) * scale
         loss.backward()
         opt.step()
     with torch.no_grad():

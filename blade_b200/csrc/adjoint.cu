@@ -300,6 +300,312 @@ __global__ void __launch_bounds__(256) loss_sum_kernel(const double* __restrict_
     if (threadIdx.x == 0) *loss = -sh[0];
 }
 
+// ---- tensor-core path (P = 2, A <= 32, B <= 32, T a multiple of 128) ----------
+// Per CTA one channel f and one chunk of 128-sample tiles, both polarisations; the
+// phases of a tile run in order, separated by barriers:
+//  1. every thread converts its voltages (loaded during the previous tile's
+//     gradient MMAs) into FP16 hi/lo pairs and stores two operand forms:
+//       XF[p][h]  128 rows (sample s) x K = [Re x | Im x] of 32 antennas,
+//       XG[h]     128 rows m = 64 p + 2 a + c (c = 0: Re, 1: Im) x K = 128 samples,
+//     both K-major with the 128-byte swizzle;
+//  2. one thread issues the forward y = x w per polarisation against the hi/lo
+//     phasor image of blade_beamform_tc_prepare (its stacked layout: hi and lo
+//     products side by side along N) for x hi and for x lo, FP32 accumulators in
+//     tensor memory;
+//  3. warps 0-3 (lane = sample) read y = hi + lo, add |y|^2 to the loss, split y into
+//     FP16 hi/lo and store YG[h]: 4 NB rows n = 2 NB p + NB c + b x K = 128 samples;
+//  4. one thread issues G += XG YG^T for the four (x, y) hi/lo combinations: M = 128
+//     rows (both polarisations), N = 4 NB, K = 128, accumulated over the chunk in
+//     tensor memory (the cross-polarisation blocks are computed and never read).
+// At the end lanes 2 a and 2 a + 1 of warp quarter p hold, for every beam, the four
+// real products of (Re x_a, Im x_a) with (Re y_b, Im y_b); one lane shuffle gives
+//   Re G = Re x . Re y + Im x . Im y,   Im G = Re x . Im y - Im x . Re y,
+// and G = sum_t y conj(x) per chunk goes to the partial sums that the two reduction
+// kernels above add in a fixed order.  The phases wait on tcgen05 commits with
+// bounded waits; on expiry the kernel records a status and returns.
+constexpr int kTcThreads = 256;
+constexpr uint32_t kTcKA = 32;
+constexpr long long kTcBudget = 2000000000ll;
+
+struct AdjTcArgs {
+    const float4* x;      // [A][F][T] (p0 re, p0 im, p1 re, p1 im)
+    const uint8_t* plan;  // phasor images, img_bytes per channel
+    float4* gpart;        // [gridDim.x][B A]
+    double* lpart;        // [gridDim.x]
+    uint32_t A, B, F, T, NB, img_bytes, nch, tiles_per_chunk;
+};
+
+__device__ unsigned int g_adj_status = 0;
+
+__device__ __forceinline__ uint32_t split_pair(float v0, float v1, uint32_t& lo) {
+    const __half h0 = __float2half_rn(v0), h1 = __float2half_rn(v1);
+    const __half l0 = __float2half_rn(v0 - __half2float(h0)), l1 = __float2half_rn(v1 - __half2float(h1));
+    lo = (uint32_t)__half_as_ushort(l0) | ((uint32_t)__half_as_ushort(l1) << 16);
+    return (uint32_t)__half_as_ushort(h0) | ((uint32_t)__half_as_ushort(h1) << 16);
+}
+
+// Byte offset of K element k (k even for 4-byte pairs) of `row` in a K-major 128-byte-
+// swizzled operand whose 64-element K blocks are `block_bytes` apart.
+__device__ __forceinline__ uint32_t kmaj_off(uint32_t row, uint32_t k, uint32_t block_bytes) {
+    return (k >> 6) * block_bytes + tc::sw128_off(row, (k >> 3) & 7u) + (k & 7u) * 2u;
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) adjoint_tc_kernel(const AdjTcArgs g) {
+    using namespace tc;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    const uint32_t NB = g.NB, A = g.A, F = g.F, T = g.T;
+    const uint32_t img_pad = (g.img_bytes + 1023u) & ~1023u;
+    uint8_t* img = smem;
+    uint8_t* xf = img + img_pad;          // [p][h] 16 KB each
+    uint8_t* xg = xf + 4 * 16384;         // [h] 32 KB each (two K blocks of 16 KB)
+    uint8_t* yg = xg + 2 * 32768;         // [h] 2 K blocks of 4 NB rows x 128 B
+    const uint32_t yblk = 4u * NB * 128u, yg_h = 2u * yblk;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(yg + 2 * yg_h);  // bar_f, bar_g, bar_end
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3);
+    double* red = reinterpret_cast<double*>(xf);  // loss reduction, after the last MMA has drained
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    volatile int never = 0;
+
+    const uint32_t f = blockIdx.x / g.nch, chunk = blockIdx.x - f * g.nch;
+    const uint32_t ntiles = T / 128u;
+    const uint32_t tile0 = chunk * g.tiles_per_chunk, tile1 = min(ntiles, tile0 + g.tiles_per_chunk);
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init(&bars[2], 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(tmem_slot, 512);
+        tmem_relinquish();
+    }
+    // the channel's phasor image and zero voltage operands (padded antennas stay 0)
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(g.plan + (uint64_t)f * g.img_bytes);
+        uint4* dst = reinterpret_cast<uint4*>(img);
+        for (uint32_t i = tid; i < g.img_bytes / 16; i += kTcThreads) dst[i] = src[i];
+        uint4* z = reinterpret_cast<uint4*>(xf);
+        for (uint32_t i = tid; i < (4 * 16384 + 2 * 32768) / 16; i += kTcThreads) z[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t d_cols = 4u * NB;           // forward accumulator columns per polarisation
+    const uint32_t dg = tmem + 256u;           // gradient accumulator, columns 256 .. 256 + 4 NB
+    const uint32_t idesc_f = idesc_f16(128, d_cols), idesc_g = idesc_f16(128, 4u * NB);
+
+    // voltages of this thread's tasks: (antenna pair a2, sample pair s2) = (t / 64, t % 64)
+    float4 xv[4][4];  // [task][(a0, s0), (a0, s0 + 1), (a0 + 1, s0), (a0 + 1, s0 + 1)]
+    auto load = [&](uint32_t tile) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint32_t tk = tid + kTcThreads * i, a0 = 2u * (tk >> 6), s0 = 2u * (tk & 63u);
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const uint32_t a = a0 + (e >> 1), s = s0 + (e & 1);
+                xv[i][e] = a < A ? __ldg(g.x + ((uint64_t)a * F + f) * T + tile * 128u + s)
+                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+    };
+    double lsum = 0.0;
+    uint32_t fph = 0, gph = 0;
+    bool ok = true;
+    if (tile0 < tile1) load(tile0);
+    for (uint32_t tile = tile0; tile < tile1 && ok; tile++) {
+        // the previous tile's gradient MMAs read XF/XG/YG: wait for them
+        if (tile > tile0) {
+            const bool w = mbar_wait(&bars[1], gph, &never, kTcBudget);
+            gph ^= 1;
+            if (!__syncthreads_and(w)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+        }
+        // phase 1: operands
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint32_t tk = tid + kTcThreads * i, a0 = 2u * (tk >> 6), s0 = 2u * (tk & 63u);
+            if (a0 >= kTcKA) continue;
+#pragma unroll
+            for (int p = 0; p < 2; p++) {
+#pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    // component (p, c) of the four samples: v[a][s]
+                    float v[2][2];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const float4 q = xv[i][e];
+                        v[e >> 1][e & 1] = p ? (c ? q.w : q.z) : (c ? q.y : q.x);
+                    }
+                    // XF: row s, K = 32 c + a0 (antennas a0, a0 + 1)
+#pragma unroll
+                    for (int ds = 0; ds < 2; ds++) {
+                        uint32_t lo;
+                        const uint32_t hi = split_pair(v[0][ds], v[1][ds], lo);
+                        const uint32_t off = kmaj_off(s0 + ds, 32u * c + a0, 16384u);
+                        *reinterpret_cast<uint32_t*>(xf + (2 * p + 0) * 16384 + off) = hi;
+                        *reinterpret_cast<uint32_t*>(xf + (2 * p + 1) * 16384 + off) = lo;
+                    }
+                    // XG: row 64 p + 2 a + c, K = s0 (samples s0, s0 + 1)
+#pragma unroll
+                    for (int da = 0; da < 2; da++) {
+                        uint32_t lo;
+                        const uint32_t hi = split_pair(v[da][0], v[da][1], lo);
+                        const uint32_t off = kmaj_off(64u * p + 2u * (a0 + da) + c, s0, 16384u);
+                        *reinterpret_cast<uint32_t*>(xg + off) = hi;
+                        *reinterpret_cast<uint32_t*>(xg + 32768 + off) = lo;
+                    }
+                }
+            }
+        }
+        fence_proxy_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        // phase 2: forward, x hi and x lo against the stacked hi/lo image
+        if (tid == 0) {
+            const uint64_t wdesc = smem_desc_sw128(smem_u32(img));
+            const uint32_t wpol16 = 4u * NB * 8u;  // one polarisation's column block of 4 NB rows
+#pragma unroll 1
+            for (uint32_t p = 0; p < 2; p++) {
+                const uint32_t d = tmem + p * d_cols;
+#pragma unroll 1
+                for (uint32_t h = 0; h < 2; h++) {
+                    const uint64_t ad = smem_desc_sw128(smem_u32(xf + (2 * p + h) * 16384));
+                    for (uint32_t j = 0; j < 4; j++)
+                        mma_f16(d, ad + (uint64_t)((j * 32u) >> 4), wdesc + (uint64_t)(p * wpol16 + j * 2u), idesc_f,
+                                (h | j) ? 1u : 0u);
+                }
+            }
+            mma_commit(&bars[0]);
+        }
+        // the next tile's voltages travel while the tensor cores work
+        if (tile + 1 < tile1) load(tile + 1);
+        {
+            const bool w = mbar_wait(&bars[0], fph, &never, kTcBudget);
+            fph ^= 1;
+            if (!__syncthreads_and(w)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+        }
+        // phase 3: y (lane = sample) -> loss and the YG operand
+        if (warp < 4) {
+            const uint32_t s = 32u * warp + lane;
+            const uint32_t lane_addr = tmem + ((32u * warp) << 16);
+            float lt = 0.f;
+            for (uint32_t p = 0; p < 2; p++) {
+                for (uint32_t b0 = 0; b0 < NB; b0 += 16) {
+                    uint32_t hr[16], hi_[16], lr[16], li[16];
+                    tmem_ld16(lane_addr + p * d_cols + b0, hr);
+                    tmem_ld16(lane_addr + p * d_cols + NB + b0, hi_);
+                    tmem_ld16(lane_addr + p * d_cols + 2 * NB + b0, lr);
+                    tmem_ld16(lane_addr + p * d_cols + 3 * NB + b0, li);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int e = 0; e < 16; e++) {
+                        const float yr = __uint_as_float(hr[e]) + __uint_as_float(lr[e]);
+                        const float yi = __uint_as_float(hi_[e]) + __uint_as_float(li[e]);
+                        lt = fmaf(yr, yr, fmaf(yi, yi, lt));
+                        const uint32_t b = b0 + e;
+#pragma unroll
+                        for (int c = 0; c < 2; c++) {
+                            const float v = c ? yi : yr;
+                            const __half h = __float2half_rn(v);
+                            const __half l = __float2half_rn(v - __half2float(h));
+                            const uint32_t off = kmaj_off(2u * NB * p + NB * c + b, s, yblk);
+                            *reinterpret_cast<__half*>(yg + off) = h;
+                            *reinterpret_cast<__half*>(yg + yg_h + off) = l;
+                        }
+                    }
+                }
+            }
+            lsum += (double)lt;
+        }
+        fence_proxy_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        // phase 4: G += XG YG^T over the four hi/lo combinations, accumulated over the chunk
+        if (tid == 0) {
+            for (uint32_t hx = 0; hx < 2; hx++)
+                for (uint32_t hy = 0; hy < 2; hy++) {
+                    const uint64_t ad = smem_desc_sw128(smem_u32(xg + hx * 32768));
+                    const uint64_t bd = smem_desc_sw128(smem_u32(yg + hy * yg_h));
+                    for (uint32_t j = 0; j < 8; j++) {
+                        const uint32_t first = (tile == tile0 && hx == 0 && hy == 0 && j == 0) ? 1u : 0u;
+                        mma_f16(dg, ad + (uint64_t)(((j >> 2) * 16384u + (j & 3u) * 32u) >> 4),
+                                bd + (uint64_t)(((j >> 2) * yblk + (j & 3u) * 32u) >> 4), idesc_g, first ? 0u : 1u);
+                    }
+                }
+            mma_commit(&bars[1]);
+        }
+    }
+    // drain: every MMA this CTA issued has completed before tensor memory is read or freed
+    if (tid == 0) {
+        mma_commit(&bars[2]);
+        if (!mbar_wait(&bars[2], 0, &never, kTcBudget)) atomicCAS(&g_adj_status, 0u, 2u);
+    }
+    if (!ok && tid == 0) atomicCAS(&g_adj_status, 0u, 1u);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    // final: G of this chunk, lanes (2 a, 2 a + 1) of quarter 2 p + a / 16
+    if (warp < 4 && ok && tile0 < tile1) {
+        const uint32_t m = 32u * warp + lane, p = m >> 6, a = (m & 63u) >> 1;
+        const bool re_lane = (m & 1u) == 0;
+        const uint32_t lane_addr = dg + ((32u * warp) << 16);
+        const uint32_t Q = g.B * A;
+        for (uint32_t b0 = 0; b0 < NB; b0 += 16) {
+            uint32_t ur[16], vr[16];
+            tmem_ld16(lane_addr + 2u * NB * p + b0, ur);       // x_c . Re y_b
+            tmem_ld16(lane_addr + 2u * NB * p + NB + b0, vr);  // x_c . Im y_b
+            tmem_ld_wait();
+#pragma unroll
+            for (int e = 0; e < 16; e++) {
+                const float u = __uint_as_float(ur[e]), v = __uint_as_float(vr[e]);
+                const float u1 = __shfl_xor_sync(0xffffffffu, u, 1), v1 = __shfl_xor_sync(0xffffffffu, v, 1);
+                const uint32_t b = b0 + e;
+                if (re_lane && a < A && b < g.B) {
+                    // lane 2a: (Re x . Re y, Re x . Im y); lane 2a + 1: (Im x . Re y, Im x . Im y)
+                    float2* gp = reinterpret_cast<float2*>(g.gpart + (uint64_t)blockIdx.x * Q + b * A + a);
+                    gp[p] = make_float2(u + v1, v - u1);
+                }
+            }
+        }
+    } else if (warp < 4 && tile0 >= tile1) {
+        // an empty chunk contributes zeros
+        const uint32_t m = 32u * warp + lane, p = m >> 6, a = (m & 63u) >> 1;
+        if ((m & 1u) == 0 && a < A)
+            for (uint32_t b = 0; b < g.B; b++)
+                reinterpret_cast<float2*>(g.gpart + (uint64_t)blockIdx.x * g.B * A + b * A + a)[p] = make_float2(0.f, 0.f);
+    }
+    red[tid] = lsum;
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 512);
+    }
+    for (uint32_t s = kTcThreads / 2; s > 0; s >>= 1) {
+        if (tid < s) red[tid] += red[tid + s];
+        __syncthreads();
+    }
+    if (tid == 0) g.lpart[blockIdx.x] = red[0];
+}
+
+size_t adjoint_tc_smem(uint32_t NB, uint32_t img_bytes) {
+    const size_t img_pad = (img_bytes + 1023u) & ~1023u;
+    return 1024 + img_pad + 4 * 16384 + 2 * 32768 + 2 * (2u * 4u * NB * 128u) + 4 * 8;
+}
+
 // Stream-ordered scratch comes from a pool owned by the library, one per device,
 // that keeps its memory between calls (release threshold = max): steady-state
 // calls reuse it and never reach the driver's allocator, which the default pool
@@ -337,6 +643,77 @@ cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
 }  // namespace
 }  // namespace bb
 
+namespace bb {
+
+// Reads and clears the adjoint kernels' device status word (blade_device_status).
+int adjoint_status_take(uint32_t* v) {
+    unsigned int x = 0, zero = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&x, g_adj_status, sizeof(x));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_adj_status, &zero, sizeof(zero));
+    if (e != cudaSuccess) return check_cuda(e, "blade_device_status");
+    *v = x;
+    return BLADE_SUCCESS;
+}
+
+namespace {
+
+bool adjoint_tc_applies(uint64_t B, uint64_t A, uint64_t F, uint64_t T, uint64_t P, const void* in) {
+    return P == 2 && A >= 1 && A <= kTcKA && B >= 1 && B <= 32 && T > 0 && T % 128 == 0 && T < (1ull << 31) &&
+           F > 0 && F < (1ull << 24) && aligned16(in);
+}
+
+int adjoint_tensor_cores(const void* in, const void* phasors, void* grad, double* loss, uint64_t B, uint64_t A,
+                         uint64_t F, uint64_t T, cudaStream_t s) {
+    const char* who = "blade_beamform_detect_adjoint";
+    const uint32_t NB = (uint32_t)((B + 15) / 16 * 16);
+    const uint32_t img_bytes = 1024u * NB;  // stacked image of 32 antennas (blade_beamform_tc_prepare)
+    const uint64_t plan_bytes = blade_beamform_tc_plan_size(B, A, F, 2);
+    if (plan_bytes != (uint64_t)F * img_bytes) return set_error(BLADE_ASSERTION_ERROR, "%s: image layout", who);
+    const uint64_t ntiles = T / 128, Q = B * A;
+    uint64_t nch = (uint64_t)sm_count() / F;  // one CTA per SM (all of tensor memory)
+    if (nch < 1) nch = 1;
+    if (nch > ntiles) nch = ntiles;
+    const uint64_t tpc = (ntiles + nch - 1) / nch;
+    nch = (ntiles + tpc - 1) / tpc;
+    const size_t smem = adjoint_tc_smem(NB, img_bytes);
+    if (int rc = ensure_smem(reinterpret_cast<const void*>(adjoint_tc_kernel), smem)) return rc;
+    uint8_t* plan = nullptr;
+    float4* gpart = nullptr;
+    double* lpart = nullptr;
+    cudaError_t e = scratch_alloc(reinterpret_cast<void**>(&plan), plan_bytes, s);
+    if (e == cudaSuccess) e = scratch_alloc(reinterpret_cast<void**>(&gpart), F * nch * Q * sizeof(float4), s);
+    if (e == cudaSuccess) e = scratch_alloc(reinterpret_cast<void**>(&lpart), F * nch * sizeof(double), s);
+    int rc = e == cudaSuccess ? BLADE_SUCCESS : check_cuda(e, "blade_beamform_detect_adjoint (scratch)");
+    if (!rc) rc = blade_beamform_tc_prepare(phasors, plan, B, A, F, 2, reinterpret_cast<blade_stream_t>(s));
+    if (!rc) {
+        AdjTcArgs g;
+        g.x = static_cast<const float4*>(in);
+        g.plan = plan;
+        g.gpart = gpart;
+        g.lpart = lpart;
+        g.A = (uint32_t)A;
+        g.B = (uint32_t)B;
+        g.F = (uint32_t)F;
+        g.T = (uint32_t)T;
+        g.NB = NB;
+        g.img_bytes = img_bytes;
+        g.nch = (uint32_t)nch;
+        g.tiles_per_chunk = (uint32_t)tpc;
+        adjoint_tc_kernel<<<(unsigned)(F * nch), kTcThreads, smem, s>>>(g);
+        adjoint_chunks_kernel<<<grid_for(F * Q, 256), 256, 0, s>>>(gpart, static_cast<float2*>(grad), (uint32_t)B,
+                                                                   (uint32_t)A, (uint32_t)F, (uint32_t)nch);
+        if (loss) loss_sum_kernel<<<1, 256, 0, s>>>(lpart, (uint32_t)(F * nch), loss);
+        rc = check_launch(who);
+    }
+    if (plan) cudaFreeAsync(plan, s);
+    if (gpart) cudaFreeAsync(gpart, s);
+    if (lpart) cudaFreeAsync(lpart, s);
+    return rc;
+}
+
+}  // namespace
+}  // namespace bb
+
 extern "C" int blade_beamform_detect_adjoint(const void* in, const void* phasors, void* grad, double* loss, uint64_t B,
                                              uint64_t A, uint64_t F, uint64_t T, uint64_t P, blade_stream_t stream) {
     using namespace bb;
@@ -345,6 +722,36 @@ extern "C" int blade_beamform_detect_adjoint(const void* in, const void* phasors
     if (!in || !phasors || !grad) return set_error(BLADE_ERROR, "blade_beamform_detect_adjoint: null buffer");
     if (F * P > 0x7fffffffull || T >= (1ull << 32) || T == 0)
         return set_error(BLADE_ERROR, "blade_beamform_detect_adjoint: dimensions out of range");
+    // below 8 beams the contraction is GEMV-like and the CUDA-core kernel, bound by the
+    // voltage read, is faster (B = 1: 58 us against 222 us on the calibration block)
+    if (B >= 8 && adjoint_tc_applies(B, A, F, T, P, in))
+        return adjoint_tensor_cores(in, phasors, grad, loss, B, A, F, T, reinterpret_cast<cudaStream_t>(stream));
+    return blade_beamform_detect_adjoint_f32(in, phasors, grad, loss, B, A, F, T, P, stream);
+}
+
+extern "C" int blade_beamform_detect_adjoint_tc(const void* in, const void* phasors, void* grad, double* loss,
+                                                uint64_t B, uint64_t A, uint64_t F, uint64_t T, uint64_t P,
+                                                blade_stream_t stream) {
+    using namespace bb;
+    if (B == 0 || A == 0 || F == 0) return BLADE_SUCCESS;
+    if (!in || !phasors || !grad) return set_error(BLADE_ERROR, "blade_beamform_detect_adjoint_tc: null buffer");
+    if (!adjoint_tc_applies(B, A, F, T, P, in))
+        return set_error(BLADE_ERROR,
+                         "blade_beamform_detect_adjoint_tc: needs P = 2, 1 <= A <= 32, 1 <= B <= 32, T %% 128 == 0 "
+                         "and 16-byte aligned voltages (B=%llu A=%llu T=%llu P=%llu)",
+                         (unsigned long long)B, (unsigned long long)A, (unsigned long long)T, (unsigned long long)P);
+    return adjoint_tensor_cores(in, phasors, grad, loss, B, A, F, T, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int blade_beamform_detect_adjoint_f32(const void* in, const void* phasors, void* grad, double* loss,
+                                                 uint64_t B, uint64_t A, uint64_t F, uint64_t T, uint64_t P,
+                                                 blade_stream_t stream) {
+    using namespace bb;
+    if (P != 1 && P != 2) return set_error(BLADE_ERROR, "blade_beamform_detect_adjoint_f32: P must be 1 or 2");
+    if (B == 0 || A == 0 || F == 0) return BLADE_SUCCESS;
+    if (!in || !phasors || !grad) return set_error(BLADE_ERROR, "blade_beamform_detect_adjoint_f32: null buffer");
+    if (F * P > 0x7fffffffull || T >= (1ull << 32) || T == 0)
+        return set_error(BLADE_ERROR, "blade_beamform_detect_adjoint_f32: dimensions out of range");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const uint64_t Q = B * A;
     const size_t fast_smem = 16 + (Q + A * (kTA + 1) + B * kTA + kTA) * sizeof(float4) + kTA * sizeof(double);

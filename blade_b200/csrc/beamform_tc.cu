@@ -1601,12 +1601,20 @@ extern "C" int blade_beamform_prepare_detect_tc_cf16(const void* phasors, void* 
                   pick_cf16(integration), stream, true);
 }
 
+namespace bb {
+int adjoint_status_take(uint32_t* v);
+}
+
 extern "C" int blade_device_status(uint32_t* status) {
     unsigned int v = 0, zero = 0;
     cudaError_t e = cudaMemcpyFromSymbol(&v, g_tc_status, sizeof(v));
     if (e != cudaSuccess) return check_cuda(e, "blade_device_status");
     e = cudaMemcpyToSymbol(g_tc_status, &zero, sizeof(zero));
     if (e != cudaSuccess) return check_cuda(e, "blade_device_status");
+    // the tensor-core adjoint's word: codes 0x100 | 1 (a phase wait expired), 0x100 | 2 (the drain did)
+    uint32_t adj = 0;
+    if (int rc = bb::adjoint_status_take(&adj)) return rc;
+    if (!v && adj) v = 0x100u | adj;
     if (status) *status = v;
     return BLADE_SUCCESS;
 }

@@ -414,6 +414,23 @@ BLADE_API int blade_beamform_detect_adjoint(const void* in, const void* phasors,
                                   double* loss, uint64_t B, uint64_t A, uint64_t F,
                                   uint64_t T, uint64_t P, blade_stream_t stream);
 
+/* The same gradient and loss on tensor cores: per 128-sample tile the forward
+ * y = x w and the contraction over time G += y conj(x) as tcgen05 MMAs with FP16
+ * hi/lo splits of voltages, weights and beams and FP32 accumulation in tensor
+ * memory; the beams are recomputed per tile and never stored.  Needs P = 2,
+ * A <= 32, B <= 32, T % 128 == 0 and 16-byte aligned voltages (else BLADE_ERROR). */
+BLADE_API int blade_beamform_detect_adjoint_tc(const void* in, const void* phasors, void* grad,
+                                     double* loss, uint64_t B, uint64_t A, uint64_t F,
+                                     uint64_t T, uint64_t P, blade_stream_t stream);
+
+/* The same gradient and loss on CUDA cores in FP32, for every shape.
+ * blade_beamform_detect_adjoint takes the tensor-core path for 8 <= B and the
+ * shapes it supports, this one otherwise (below 8 beams the contraction is
+ * GEMV-like and bound by the voltage read, where this kernel is faster). */
+BLADE_API int blade_beamform_detect_adjoint_f32(const void* in, const void* phasors, void* grad,
+                                      double* loss, uint64_t B, uint64_t A, uint64_t F,
+                                      uint64_t T, uint64_t P, blade_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
