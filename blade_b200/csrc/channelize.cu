@@ -19,8 +19,10 @@
 // to the output.
 #include "autotune.cuh"
 #include "common.cuh"
+#include "tc_ptx.cuh"
 
 namespace bb {
+
 namespace {
 
 constexpr int kThreads = 256;
@@ -53,8 +55,10 @@ bool make_plan(uint64_t N, Plan& p) {
     return true;
 }
 
+// Complex product with its two fused multiply-adds spelled out, so that every
+// kernel rounds it the same way whatever the compiler would contract.
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    return make_float2(fmaf(a.x, b.x, -(a.y * b.y)), fmaf(a.x, b.y, a.y * b.x));
 }
 // Complex add and subtract as one packed FP32x2 instruction each (both lanes round
 // as the scalar add would; a - b is fma(b, -1, a), whose product is exact).
@@ -439,6 +443,8 @@ __global__ void __launch_bounds__(256, 2) fft8192_kernel(const float2* __restric
         const uint64_t af = as / S;
         const uint32_t s = (uint32_t)(as - af * S);
         const float2* src = in + as * (uint64_t)kN8 * P + p;  // sample n at src[n P]
+        if (tid < 16 && unit + gridDim.x < units)  // the next unit's spectrum into L2 while this one runs
+            tc::prefetch_l2_bulk(in + ((unit + gridDim.x) / P) * (uint64_t)kN8 * P + 512 * P * tid, 4096u * P);
         // stage A: columns t = tid, tid + 256
 #pragma unroll 1
         for (uint32_t c = 0; c < 2; c++) {
@@ -891,16 +897,16 @@ extern "C" int blade_channelize(const void* in, void* out, void* workspace, uint
     if (rate == kN8) {
         const uint64_t units = A * F * S * P;
         const size_t smem = 16 * kZ1 * sizeof(float2);
+        const uint64_t cap = (uint64_t)sm_count() * 2;
+        const unsigned grid = (unsigned)(units < cap ? units : cap);
         int rc;
         if (P == 2) {
             if ((rc = prepare_smem(fft8192_kernel<2>, smem))) return rc;
+            fft8192_kernel<2><<<grid, 256, smem, s>>>(src, dst, units, (uint32_t)S);
         } else {
             if ((rc = prepare_smem(fft8192_kernel<1>, smem))) return rc;
+            fft8192_kernel<1><<<grid, 256, smem, s>>>(src, dst, units, (uint32_t)S);
         }
-        const uint64_t cap = (uint64_t)sm_count() * 2;
-        const unsigned grid = (unsigned)(units < cap ? units : cap);
-        if (P == 2) fft8192_kernel<2><<<grid, 256, smem, s>>>(src, dst, units, (uint32_t)S);
-        else fft8192_kernel<1><<<grid, 256, smem, s>>>(src, dst, units, (uint32_t)S);
         return check_launch("blade_channelize");
     }
     if (!workspace) return set_error(BLADE_ERROR, "blade_channelize: rate %llu needs a workspace of %llu bytes",

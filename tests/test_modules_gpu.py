@@ -125,7 +125,7 @@ CH_CASES = [
     (4, 6, 64, 2, 4),
     (2, 3, 96, 2, 6),
     (2, 5, 4096, 2, 4096),
-    (1, 2, 16384, 2, 8192),     # four-step path
+    (1, 2, 16384, 2, 8192),     # rate 8192, two spectra per row
     (1, 2, 131072, 2, 65536),   # the spectrometer NFFT
     (3, 4, 20, 2, 2),
     # rates 2, 4, 8, 16 run one spectrum per thread in registers: both pol counts
@@ -136,6 +136,7 @@ CH_CASES = [
     (2, 3, 512, 1, 16),
     (2, 2, 64, 1, 2),
     (2, 3, 24576, 1, 8192),     # rate 8192: one transform per CTA unit, three spectra per row
+    (2, 3, 24576, 2, 8192),     # rate 8192, two polarisations, three spectra per row
 ]
 
 
@@ -159,6 +160,25 @@ def test_channelizer_in_place_rate_equals_T(cuda, A, F, T, P):
     xd = c64(x)
     call("blade_channelize", ptr(xd), ptr(xd), None, A, F, T, P, T, stream())
     assert rel_l2(host(xd).reshape(A, F * T, 1, P), O.channelize(x, T)) < TOL
+
+
+@pytest.mark.parametrize("A,F,nspec", [(2, 3, 3), (4, 40, 1)])
+def test_rate8192_two_polarisations_match_one(cuda, A, F, nspec):
+    # At rate 8192 each CTA unit is one polarisation of one spectrum: the unit of a
+    # two-polarisation input computes exactly what the one-polarisation input of that
+    # polarisation does (bit for bit).  160 x 2 units (the second case) make each CTA
+    # loop, prefetching its next unit's spectrum into L2.
+    T = 8192 * nspec
+    rng = np.random.default_rng(8192 + A * F * nspec)
+    x = crand(rng, (A, F, T, 2))
+    y = torch.zeros((A, F * 8192, nspec, 2), dtype=torch.complex64, device="cuda")
+    call("blade_channelize", ptr(c64(x)), ptr(y), None, A, F, T, 2, 8192, stream())
+    for p in range(2):
+        xp = c64(np.ascontiguousarray(x[..., p:p + 1]))
+        yp = torch.zeros((A, F * 8192, nspec, 1), dtype=torch.complex64, device="cuda")
+        call("blade_channelize", ptr(xp), ptr(yp), None, A, F, T, 1, 8192, stream())
+        assert torch.equal(y[..., p:p + 1], yp)
+    assert rel_l2(host(y), O.channelize(x, 8192)) < TOL
 
 
 # ------------------------------------------------------------------------ polarizer
