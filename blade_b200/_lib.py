@@ -68,6 +68,7 @@ _SIGNATURES = {
     "blade_beamform_detect_adjoint_f32": (_int, [_vp, _vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp]),
     "blade_beamform_detect_adjoint_tc": (_int, [_vp, _vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp]),
     "blade_device_status": (_int, [C.POINTER(C.c_uint32)]),
+    "blade_wait_selftest": (_int, [_u64, _vp]),
     "blade_beamform_detect_tc_noalloc": (_int, [_vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),
     "blade_beamform_detect_tc_autotune": (_int, [_u64, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),
     "blade_beamform_detect_f32_autotune": (_int, [_int, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _vp]),

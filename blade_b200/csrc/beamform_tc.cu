@@ -1619,6 +1619,37 @@ extern "C" int blade_device_status(uint32_t* status) {
     return BLADE_SUCCESS;
 }
 
+// ---- bounded-wait self-test ---------------------------------------------------
+// One thread waits on an mbarrier that nothing ever completes, through the same
+// bounded wait as the pipelined kernels; when the budget runs out it records
+// kSelftestCode in the status word and the kernel returns normally, so the
+// expiry path is exercised without a fault and the context stays usable.
+namespace bb {
+namespace {
+constexpr unsigned kSelftestCode = 0x20u;
+
+__global__ void wait_selftest_kernel(long long budget) {
+    __shared__ __align__(8) uint64_t bar;
+    volatile int never = 0;
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&bar, 1);  // one arrival completes phase 0; none is ever made
+        tc::fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && !tc::mbar_wait(&bar, 0, &never, budget)) atomicCAS(&g_tc_status, 0u, kSelftestCode);
+}
+}  // namespace
+}  // namespace bb
+
+extern "C" int blade_wait_selftest(uint64_t budget_cycles, blade_stream_t stream) {
+    using namespace bb;
+    if (budget_cycles == 0 || budget_cycles > 10000000000ull)
+        return set_error(BLADE_ERROR, "blade_wait_selftest: budget must be 1 .. 1e10 cycles (got %llu)",
+                         (unsigned long long)budget_cycles);
+    wait_selftest_kernel<<<1, 32, 0, reinterpret_cast<cudaStream_t>(stream)>>>((long long)budget_cycles);
+    return check_launch("blade_wait_selftest");
+}
+
 // ---- allocation-free variant ---------------------------------------------------
 // For callers that must not allocate device memory while they stream: an online
 // beamformer that sizes its whole GPU budget once at start-up and then runs a

@@ -297,6 +297,13 @@ BLADE_API int blade_incoherent_detect_cf16(const void* in, const void* phasors, 
  * ------------------------------------------------------------------------- */
 BLADE_API int blade_device_status(uint32_t* status);
 
+/* Exercises the expiry path of those bounded waits: one thread waits on a barrier
+ * that nothing completes, gives up after budget_cycles SM clock cycles (1 .. 1e10)
+ * and records status 0x20, which the next blade_device_status() returns; the
+ * kernel itself returns normally, and later launches are unaffected.  No
+ * reference counterpart (a health check for callers that monitor the status). */
+BLADE_API int blade_wait_selftest(uint64_t budget_cycles, blade_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Geometric delays: the astrometric half of Modules::Phasor::ATA::process
  * (src/modules/phasor/ata.cc:9-173; the reference calls ERFA through

@@ -191,3 +191,29 @@ def test_adjoint_general_path_vs_fp64(cuda, A, F, T, B, P):
     call("blade_beamform_detect_adjoint", ptr(xd), ptr(wd), ptr(gd), ptr(ld), B, A, F, T, P, stream())
     assert rel_l2(host(gd), O.stokes_loss_grad(x, w)) < TOL
     assert abs(host(ld)[0] - O.stokes_loss(x, w)) / abs(O.stokes_loss(x, w)) < TOL
+
+
+def test_bounded_wait_expiry_is_reported_and_the_context_survives(cuda):
+    # A wait that nothing completes gives up after its budget (2e6 cycles, about a
+    # millisecond), records its code in the status word and returns; the status is
+    # read once and cleared, and the tensor-core chain then runs normally.
+    assert bl.device_status() == 0
+    call("blade_wait_selftest", 2_000_000, stream())
+    torch.cuda.synchronize()
+    assert bl.device_status() == 0x20
+    assert bl.device_status() == 0
+    A, F, T, B, R, I = 28, 2, 1024, 16, 4, 4
+    x, w = make(A, F, T, B, 11)
+    xd, wd = dev(x), c64(w)
+    plan = torch.empty(int(_lib.load().blade_beamform_tc_plan_size(B, A, F, 2)), dtype=torch.uint8, device="cuda")
+    od = torch.zeros((B, F * R, T // (R * I), 1), dtype=torch.float32, device="cuda")
+    call("blade_beamform_prepare_detect_tc", ptr(wd), ptr(plan), ptr(xd), ptr(od), B, A, F, T, 2, R, I, stream())
+    assert rel_l2(host(od), O.beamform_channelize_detect(x, w, R, I)) < TOL
+    assert bl.device_status() == 0
+
+
+def test_wait_selftest_rejects_bad_budgets(cuda):
+    with pytest.raises(_lib.BladeError):
+        call("blade_wait_selftest", 0, stream())
+    with pytest.raises(_lib.BladeError):
+        call("blade_wait_selftest", 10**11, stream())
