@@ -14,7 +14,9 @@
 // accumulates y conj(x) for its (beam, antenna) pairs over its slice of every tile
 // in registers.  The slices are added in a fixed order at the end, the chunks by a
 // second kernel and the loss by a third, so results are deterministic.  HBM traffic
-// is one read of the voltages.  Other shapes take the one-CTA-per-(f, p) kernel.
+// is one read of the voltages.  One beam (B = 1, A <= 32) takes a kernel without
+// shared-memory staging (adjoint_b1_kernel); other shapes the one-CTA-per-(f, p)
+// kernel.
 #include <mutex>
 
 #include "common.cuh"
@@ -298,6 +300,105 @@ __global__ void __launch_bounds__(256) loss_sum_kernel(const double* __restrict_
         __syncthreads();
     }
     if (threadIdx.x == 0) *loss = -sh[0];
+}
+
+// ---- one beam (the calibration shape: B = 1, P = 2, A <= 32) -------------------
+// No shared-memory staging: four threads share a sample, thread g of the group
+// owning antennas a = g + 4 i (i < NA); each loads its voltages with 16-byte loads
+// (both polarisations), multiplies them by its phasors (held in registers), the
+// group adds its four partial beam voltages with two lane shuffles, and every
+// thread accumulates y conj(x_a) for its own antennas in registers across the
+// chunk.  The CTA's 64 sample lanes are reduced once at the end (lane shuffles,
+// then the eight warps in a fixed order) into the same per-chunk partials as the
+// shared-memory kernel above, which the two reduction kernels add in a fixed order.
+// One read of the voltages is the only HBM traffic, and no barrier sits between a
+// round's loads and its arithmetic.
+constexpr int kB1Threads = 256;       // 64 samples x 4 antenna groups
+constexpr uint32_t kB1Samples = 512;  // samples per CTA (chunk)
+
+template <int NA>
+__global__ void __launch_bounds__(kB1Threads) adjoint_b1_kernel(const float4* __restrict__ x,
+                                                                const float2* __restrict__ w,
+                                                                float4* __restrict__ gpart, double* __restrict__ lpart,
+                                                                uint32_t A, uint32_t F, uint32_t T, uint32_t nch) {
+    constexpr uint32_t kWarps = kB1Threads / 32;
+    __shared__ float4 red[kWarps][4][NA];
+    __shared__ double lred[kB1Threads];
+    const uint32_t f = blockIdx.x / nch, c = blockIdx.x - f * nch;
+    const uint32_t tid = threadIdx.x, g = tid & 3u, sl = tid >> 2, lane = tid & 31u, warp = tid >> 5;
+    float4 wr[NA], acc[NA];
+#pragma unroll
+    for (int i = 0; i < NA; i++) {
+        const uint32_t a = g + 4u * i;
+        wr[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (a < A) {
+            const float2 w0 = w[((uint64_t)a * F + f) * 2], w1 = w[((uint64_t)a * F + f) * 2 + 1];
+            wr[i] = make_float4(w0.x, w0.y, w1.x, w1.y);
+        }
+        acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    double lsum = 0.0;
+    const uint32_t t_beg = c * kB1Samples, t_end = min(T, t_beg + kB1Samples);
+    const float4* xf = x + (uint64_t)f * T;  // x[a][f][t] float4 = both polarisations
+    const uint64_t astride = (uint64_t)F * T;
+    // every lane runs the same number of rounds (the shuffles need the whole warp);
+    // samples past the chunk read zeros and contribute nothing
+    for (uint32_t t0 = t_beg; t0 < t_end; t0 += kB1Threads / 4) {
+        const uint32_t t = t0 + sl;
+        float4 xv[NA];
+#pragma unroll
+        for (int i = 0; i < NA; i++) {
+            const uint32_t a = g + 4u * i;
+            xv[i] = (t < t_end && a < A) ? __ldg(xf + a * astride + t) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        float4 yv = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < NA; i++) {
+            const float4 xa = xv[i], wv = wr[i];
+            yv.x = fmaf(xa.x, wv.x, fmaf(-xa.y, wv.y, yv.x));
+            yv.y = fmaf(xa.x, wv.y, fmaf(xa.y, wv.x, yv.y));
+            yv.z = fmaf(xa.z, wv.z, fmaf(-xa.w, wv.w, yv.z));
+            yv.w = fmaf(xa.z, wv.w, fmaf(xa.w, wv.z, yv.w));
+        }
+#pragma unroll
+        for (uint32_t m = 1; m <= 2; m <<= 1) {
+            yv.x += __shfl_xor_sync(0xffffffffu, yv.x, m);
+            yv.y += __shfl_xor_sync(0xffffffffu, yv.y, m);
+            yv.z += __shfl_xor_sync(0xffffffffu, yv.z, m);
+            yv.w += __shfl_xor_sync(0xffffffffu, yv.w, m);
+        }
+        if (g == 0) lsum += (double)(yv.x * yv.x + yv.y * yv.y + yv.z * yv.z + yv.w * yv.w);
+#pragma unroll
+        for (int i = 0; i < NA; i++) acc[i] = cmac2(acc[i], yv, xv[i]);
+    }
+    // the warp's eight sample lanes of each antenna group, then the warps in order
+#pragma unroll
+    for (int i = 0; i < NA; i++) {
+#pragma unroll
+        for (uint32_t m = 4; m < 32; m <<= 1) {
+            acc[i].x += __shfl_xor_sync(0xffffffffu, acc[i].x, m);
+            acc[i].y += __shfl_xor_sync(0xffffffffu, acc[i].y, m);
+            acc[i].z += __shfl_xor_sync(0xffffffffu, acc[i].z, m);
+            acc[i].w += __shfl_xor_sync(0xffffffffu, acc[i].w, m);
+        }
+        if (lane < 4) red[warp][g][i] = acc[i];
+    }
+    lred[tid] = lsum;
+    __syncthreads();
+    if (tid < A) {
+        const uint32_t ga = tid & 3u, ia = tid >> 2;
+        float4 s = red[0][ga][ia];
+        for (uint32_t k = 1; k < kWarps; k++) {
+            const float4 r = red[k][ga][ia];
+            s.x += r.x; s.y += r.y; s.z += r.z; s.w += r.w;
+        }
+        gpart[(uint64_t)blockIdx.x * A + tid] = s;
+    }
+    for (uint32_t s2 = kB1Threads / 2; s2 > 0; s2 >>= 1) {
+        if (tid < s2) lred[tid] += lred[tid + s2];
+        __syncthreads();
+    }
+    if (tid == 0) lpart[blockIdx.x] = lred[0];
 }
 
 // ---- tensor-core path (P = 2, A <= 32, B <= 32, T a multiple of 128) ----------
@@ -754,6 +855,36 @@ extern "C" int blade_beamform_detect_adjoint_f32(const void* in, const void* pha
         return set_error(BLADE_ERROR, "blade_beamform_detect_adjoint_f32: dimensions out of range");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const uint64_t Q = B * A;
+    if (B == 1 && P == 2 && A <= 32 && aligned16(in)) {
+        // one beam: register-resident kernel, chunks of kB1Samples samples
+        const uint64_t nch = (T + kB1Samples - 1) / kB1Samples;
+        if (F * nch > 0x7fffffffull) return set_error(BLADE_ERROR, "blade_beamform_detect_adjoint_f32: too many chunks");
+        float4* gpart = nullptr;
+        double* lpart = nullptr;
+        cudaError_t e = scratch_alloc(reinterpret_cast<void**>(&gpart), F * nch * A * sizeof(float4), s);
+        if (e == cudaSuccess) e = scratch_alloc(reinterpret_cast<void**>(&lpart), F * nch * sizeof(double), s);
+        if (e != cudaSuccess) {
+            if (gpart) cudaFreeAsync(gpart, s);
+            return check_cuda(e, "blade_beamform_detect_adjoint (scratch)");
+        }
+        const unsigned grid = (unsigned)(F * nch);
+        const float4* x4 = static_cast<const float4*>(in);
+        const float2* w2 = static_cast<const float2*>(phasors);
+        const uint32_t a = (uint32_t)A, f = (uint32_t)F, t = (uint32_t)T, c = (uint32_t)nch;
+        switch ((A + 3) / 4) {
+#define BB_ADJ_B1(NA) \
+    case NA: adjoint_b1_kernel<NA><<<grid, kB1Threads, 0, s>>>(x4, w2, gpart, lpart, a, f, t, c); break
+            BB_ADJ_B1(1); BB_ADJ_B1(2); BB_ADJ_B1(3); BB_ADJ_B1(4);
+            BB_ADJ_B1(5); BB_ADJ_B1(6); BB_ADJ_B1(7); BB_ADJ_B1(8);
+#undef BB_ADJ_B1
+        }
+        adjoint_chunks_kernel<<<grid_for(F * Q, 256), 256, 0, s>>>(gpart, static_cast<float2*>(grad), 1u, a, f, c);
+        if (loss) loss_sum_kernel<<<1, 256, 0, s>>>(lpart, (uint32_t)(F * nch), loss);
+        const int rc = check_launch("blade_beamform_detect_adjoint");
+        cudaFreeAsync(gpart, s);
+        cudaFreeAsync(lpart, s);
+        return rc;
+    }
     const size_t fast_smem = 16 + (Q + A * (kTA + 1) + B * kTA + kTA) * sizeof(float4) + kTA * sizeof(double);
     if (P == 2 && Q <= kMaxPairs && fast_smem <= 227 * 1024 && aligned16(in)) {
         // chunks of the time axis: F * nch CTAs fill the resident slots once (one wave)
