@@ -40,7 +40,7 @@ int sm_count() {
 }
 
 int ensure_smem(const void* func, size_t bytes) {
-    if (bytes <= 48 * 1024) return BLADE_SUCCESS;
+    if (bytes == 0) return BLADE_SUCCESS;
     struct Entry { const void* f; int dev; size_t bytes; };
     static std::mutex mu;
     static std::vector<Entry> done;
@@ -49,7 +49,11 @@ int ensure_smem(const void* func, size_t bytes) {
     std::lock_guard<std::mutex> lock(mu);
     for (auto& e : done)
         if (e.f == func && e.dev == dev && e.bytes >= bytes) return BLADE_SUCCESS;
-    cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    // the 48 KB that need no opt-in cover static and dynamic shared memory together
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, func);
+    if (e == cudaSuccess && bytes + fa.sharedSizeBytes > 48 * 1024)
+        e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return set_error(BLADE_CUDA_ERROR, "shared memory opt-in (%zu bytes): %s", bytes,
                                            cudaGetErrorString(e));
     done.push_back({func, dev, bytes});
