@@ -2,8 +2,8 @@
 cores and FP16-split tcgen05 tensor cores) and of the adjoint, against the FP64
 oracle, on the workload shapes (channel count reduced so the oracle stays fast).
 
-The tensor-core path's Stokes-I error bound is the north star's 1e-5 relative L2
-against FP64; the FP32 path must meet the same bound."""
+The tensor-core path's Stokes-I error bound is 1e-5 relative L2 against FP64;
+the FP32 path must meet the same bound."""
 
 import numpy as np
 import pytest
