@@ -27,6 +27,7 @@ from .modules import (BeamformDetect, BeamformerATA, BeamformerMeerKAT, Cast, Ch
                       Gather, ModeB, ModeH, Module, Permutation, Phasor, Polarizer)
 from .runtime import Pipeline, Runner, module, runner
 from .guppi import GuppiReader, GuppiWriter
+from .bfr5 import Bfr5Reader
 
 __version__ = "1.0.0"
 

@@ -29,13 +29,13 @@ telescope_list = ["ata", "vla", "meerkat", "generic"]
 device_list = ["cpu", "cuda", "unified"]
 dtypes = ["f16", "f32", "f64", "i8", "i32", "cf16", "cf32", "cf64", "ci8"]
 module_list = ["beamformer", "cast", "channelizer", "duplicate", "detector", "gather", "permutation", "phasor",
-               "polarizer", "beamform_detect", "modeb", "modeh", "guppi_reader", "guppi_writer"]
+               "polarizer", "beamform_detect", "modeb", "modeh", "guppi_reader", "guppi_writer", "bfr5_reader"]
 
 ata, vla, meerkat, generic = (Constant(n) for n in telescope_list)
 cpu, cuda, unified = (Constant(n) for n in device_list)
 f16, f32, f64, i8, i32, cf16, cf32, cf64, ci8 = (Constant(n) for n in dtypes)
 (beamformer, cast, channelizer, duplicate, detector, gather, permutation, phasor, polarizer, beamform_detect,
- modeb, modeh, guppi_reader, guppi_writer) = (Constant(n) for n in module_list)
+ modeb, modeh, guppi_reader, guppi_writer, bfr5_reader) = (Constant(n) for n in module_list)
 
 
 class pol(enum.IntEnum):
