@@ -90,6 +90,7 @@ struct TcArgs {
     uint64_t total_tiles;
     uint32_t pdl;  // launched as a programmatic dependent of the phasor split: wait for it before the image
     uint32_t direct;  // R = 1 CI8 without a raw ring: converter threads load the voltages themselves
+    uint32_t transposed;  // outputs along TMEM lanes, samples along columns (64-beam chunks, rate 1, I = 8 or 16)
 };
 
 __device__ __forceinline__ uint32_t cvt_pair(uint32_t v) {
@@ -599,6 +600,138 @@ __device__ __forceinline__ void issue_ka32(uint32_t d, uint64_t ad, uint64_t wd,
             mma_f16(d, a_step(ad, j), wd + (uint64_t)(h * 2 * nb16 + j * 2), idesc, (h | j) ? 1u : 0u);
 }
 
+// The same products with the roles of the operands swapped: the image blocks are
+// the A operand (M = 128 rows: Re outputs of the 64 beams, then Im outputs) and the
+// tile's samples the B operand (N = 128), so the accumulator holds one output row
+// per TMEM lane and the tile's samples along its columns.
+__device__ __forceinline__ void issue_ka64_t(uint32_t d, uint64_t ad, uint64_t wd, uint32_t nb16, uint32_t idesc) {
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+            mma_f16(d, wd + (uint64_t)(h * 3 * nb16 + (j < 4 ? nb16 : 0) + (j & 3) * 2), a_step(ad, j), idesc,
+                    (h | j) ? 1u : 0u);
+}
+
+__device__ __forceinline__ void issue_ka32_t(uint32_t d, uint64_t ad, uint64_t wd, uint32_t nb16, uint32_t idesc) {
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            mma_f16(d, wd + (uint64_t)(h * 2 * nb16 + j * 2), a_step(ad, j), idesc, (h | j) ? 1u : 0u);
+}
+
+// Epilogue of the transposed accumulator (rate 1 CI8, windows of I = 8 or 16
+// samples, one 64-beam chunk): TMEM lane m holds output row m (Re of beam m for
+// m < 64, Im of beam m - 64 after) and column c sample c of the tile, so a thread
+// adds the squares of its row over each window of I consecutive columns (two
+// columns per packed FP32x2 FMA) without any lane exchange.  Warps 0 and 1 of the
+// lane quarters (the Re rows) store their window sums of both polarisations to
+// the output; warps 2 and 3 (the Im rows) keep theirs in registers and add them to
+// the stored partial sums one tile later, once pr_full says those are there.  The
+// Re half signals a tile's partial sums after reading the next tile from TMEM, so
+// neither half waits on the round trip through memory.  The Im half releases an
+// accumulator only after its wait for the previous tile, which keeps the Re half
+// within one phase of it on every pr_full barrier.
+template <int LOGI>
+__device__ __forceinline__ void epilogue_transposed(const TcArgs& g, uint32_t tmem, uint32_t d_cols, uint32_t nacc,
+                                                    uint64_t* d_full, uint64_t* d_empty, uint64_t* pr_full,
+                                                    volatile int* abort, uint64_t L0, uint64_t L1, uint32_t tpc,
+                                                    uint32_t q, uint32_t lane) {
+    constexpr uint32_t I = 1u << LOGI;
+    constexpr int NW = kM / I;                      // windows per tile: 16 or 8
+    constexpr int kCols = LOGI == 3 ? 32 : 64;      // TMEM columns read per wait
+    const bool re_half = q < 2;
+    const uint32_t b = 32u * (q & 1u) + lane;
+    const bool valid = b < g.beams;
+    const uint64_t bstride = (uint64_t)g.F * g.U;
+    uint32_t db = 0, dph = 0;
+    uint32_t f = (uint32_t)(L0 / tpc), tt = (uint32_t)(L0 % tpc);
+    float* prev = nullptr;       // output row of the previous tile, whose exchange is pending
+    uint32_t pdb = 0, pph = 0;   // its pr_full barrier and parity
+    float pend[NW];              // Im half: the previous tile's own window sums
+    bool ok = true;
+    for (uint64_t L = L0; L < L1; L++) {
+        if (!mbar_wait(&d_full[db], dph, abort, kWaitBudget)) { record_abort(abort, 7); ok = false; break; }
+        tc_fence_after();
+        const uint32_t lane_addr = tmem + ((32 * q) << 16) + db * (2 * d_cols);
+        float2 acc[NW];
+#pragma unroll
+        for (int w = 0; w < NW; w++) acc[w] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (uint32_t p = 0; p < 2; p++) {
+#pragma unroll
+            for (int c0 = 0; c0 < kM; c0 += kCols) {
+                uint32_t r[kCols / 16][16];
+#pragma unroll
+                for (int k = 0; k < kCols / 16; k++) tmem_ld16(lane_addr + p * d_cols + c0 + 16 * k, r[k]);
+                tmem_ld_wait();
+#pragma unroll
+                for (int k = 0; k < kCols / 16; k++)
+#pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        const int w = (c0 + 16 * k + 2 * j) / I;
+                        const float2 v = make_float2(__uint_as_float(r[k][2 * j]), __uint_as_float(r[k][2 * j + 1]));
+                        acc[w] = __ffma2_rn(v, v, acc[w]);
+                    }
+            }
+        }
+        tc_fence_before();
+        __syncwarp();
+        float* o = g.out + (uint64_t)b * bstride + (uint64_t)f * g.U + (uint64_t)tt * NW;
+        if (re_half) {
+            if (lane == 0) {
+                mbar_arrive(&d_empty[db]);
+                if (prev) mbar_arrive(&pr_full[pdb]);  // stored a tile ago
+            }
+            if (valid) {
+#pragma unroll
+                for (int w = 0; w < NW; w += 4)
+                    *reinterpret_cast<float4*>(o + w) = make_float4(acc[w].x + acc[w].y, acc[w + 1].x + acc[w + 1].y,
+                                                                    acc[w + 2].x + acc[w + 2].y, acc[w + 3].x + acc[w + 3].y);
+            }
+            __threadfence_block();  // ordered before lane 0's next arrive on pr_full
+            __syncwarp();
+        } else {
+            if (prev && !mbar_wait(&pr_full[pdb], pph, abort, kWaitBudget)) { record_abort(abort, 12); ok = false; break; }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&d_empty[db]);
+            if (prev && valid) {
+#pragma unroll
+                for (int w = 0; w < NW; w += 4) {
+                    const float4 r = *reinterpret_cast<const float4*>(prev + w);
+                    *reinterpret_cast<float4*>(prev + w) =
+                        make_float4(r.x + pend[w], r.y + pend[w + 1], r.z + pend[w + 2], r.w + pend[w + 3]);
+                }
+            }
+#pragma unroll
+            for (int w = 0; w < NW; w++) pend[w] = acc[w].x + acc[w].y;
+        }
+        prev = o;
+        pdb = db;
+        pph = dph;
+        if (++db == nacc) { db = 0; dph ^= 1; }
+        if (++tt == tpc) { tt = 0; f++; }
+    }
+    if (ok && prev) {
+        if (re_half) {
+            if (lane == 0) mbar_arrive(&pr_full[pdb]);
+        } else if (mbar_wait(&pr_full[pdb], pph, abort, kWaitBudget)) {
+            __syncwarp();
+            if (valid) {
+#pragma unroll
+                for (int w = 0; w < NW; w += 4) {
+                    const float4 r = *reinterpret_cast<const float4*>(prev + w);
+                    *reinterpret_cast<float4*>(prev + w) =
+                        make_float4(r.x + pend[w], r.y + pend[w + 1], r.z + pend[w + 2], r.w + pend[w + 3]);
+                }
+            }
+        } else {
+            record_abort(abort, 12);
+        }
+    }
+}
+
 // ES = bytes per dual-polarisation input sample: 4 (CI8) or 8 (CF16, rate 1 only).
 template <int R, int LOGI, int ES = 4>
 __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, const __grid_constant__ CUtensorMap tmap) {
@@ -620,7 +753,8 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
     uint64_t* w_full = d_empty + kMaxAcc;
     uint64_t* w_empty = w_full + 1;
     uint64_t* fin = w_empty + 1;  // one per MMA issuer
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fin + 2);
+    uint64_t* pr_full = fin + 2;  // transposed epilogue: the Re half's partial sums are stored
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(pr_full + kMaxAcc);
     volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -661,6 +795,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
         for (uint32_t i = 0; i < nacc; i++) {
             mbar_init(&d_full[i], 1);
             mbar_init(&d_empty[i], kEpiWarps);
+            mbar_init(&pr_full[i], kEpiWarps / 2);
         }
         mbar_init(w_full, 1);
         mbar_init(w_empty, nis);
@@ -733,6 +868,9 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
                                 if (g.stacked) {
                                     if (KA == 64) issue_stacked<8>(d, ad, wd, 4 * nb16, idesc);
                                     else issue_stacked<4>(d, ad, wd, 4 * nb16, idesc);
+                                } else if (g.transposed) {
+                                    if (KA == 64) issue_ka64_t(d, ad, wd, nb16, idesc);
+                                    else issue_ka32_t(d, ad, wd, nb16, idesc);
                                 } else if (KA == 64) {
                                     issue_ka64(d, ad, wd, nb16, idesc);
                                 } else {
@@ -854,83 +992,93 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
             __syncwarp();
         }
     } else if (warp < 2 + kEpiWarps) {
-        // ---------------- epilogue ----------------
-        constexpr uint32_t I = 1u << LOGI;
-        const uint32_t q = warp & 3;               // TMEM lane quarter this warp may access
-        const uint32_t hw = (warp - 2) >> 2;       // which share of the beams
-        const uint32_t nbh = NB / kEpiGroups;      // beams per warp, a multiple of 8
-        constexpr uint32_t rows_per_k = kM / R;
-        const uint32_t row = 32 * q + lane;
-        const uint32_t k = row / rows_per_k;
-        const uint32_t s_local = row - k * rows_per_k;
-        const uint64_t bstride = (uint64_t)g.F * R * g.U;
-        uint32_t db = 0, dph = 0;
-        uint32_t f = (uint32_t)(L0 / tpc), tt = (uint32_t)(L0 % tpc);  // stepped below
-        for (uint64_t L = L0; L < L1; L++) {
-            if (!mbar_wait(&d_full[db], dph, abort, kWaitBudget)) { record_abort(abort, 7); break; }
-            tc_fence_after();
-            const uint32_t u = (tt * rows_per_k + s_local) / I;
-            const uint32_t lane_addr = tmem + ((32 * q) << 16) + db * (2 * d_cols);
-            float* obase = g.out + ((uint64_t)f * R + k) * g.U + u;
-            constexpr int CH = 16 / kEpiGroups;  // beams per TMEM load (16 or 8)
-            for (uint32_t bc = hw * nbh; bc < (hw + 1) * nbh; bc += CH) {
-                // Two beams per packed FP32x2 instruction (each lane of the pair rounds
-                // exactly as the scalar add / multiply / FMA would).
-                float2 pw2[CH / 2];
-                float(&pw)[CH] = *reinterpret_cast<float(*)[CH]>(pw2);
-                if (g.stacked) {
-                    // per polarisation: (hi + lo) re, (hi + lo) im
-#pragma unroll
-                    for (int j = 0; j < CH; j++) pw[j] = 0.f;
-#pragma unroll
-                    for (uint32_t p = 0; p < 2; p++) {
-                        uint32_t hr[CH], hi[CH], lr[CH], li[CH];
-                        const uint32_t pa = lane_addr + p * d_cols + bc;
-                        tmem_ld(pa, hr);
-                        tmem_ld(pa + NB, hi);
-                        tmem_ld(pa + 2 * NB, lr);
-                        tmem_ld(pa + 3 * NB, li);
+        bool done = false;
+        if constexpr (R == 1 && (LOGI == 3 || LOGI == 4) && ES == 4 && kEpiWarps == 4) {
+            if (g.transposed) {
+                epilogue_transposed<LOGI>(g, tmem, d_cols, nacc, d_full, d_empty, pr_full, abort, L0, L1, tpc,
+                                          (uint32_t)(warp & 3), (uint32_t)lane);
+                done = true;
+            }
+        }
+        if (!done) {
+            // ---------------- epilogue ----------------
+            constexpr uint32_t I = 1u << LOGI;
+            const uint32_t q = warp & 3;               // TMEM lane quarter this warp may access
+            const uint32_t hw = (warp - 2) >> 2;       // which share of the beams
+            const uint32_t nbh = NB / kEpiGroups;      // beams per warp, a multiple of 8
+            constexpr uint32_t rows_per_k = kM / R;
+            const uint32_t row = 32 * q + lane;
+            const uint32_t k = row / rows_per_k;
+            const uint32_t s_local = row - k * rows_per_k;
+            const uint64_t bstride = (uint64_t)g.F * R * g.U;
+            uint32_t db = 0, dph = 0;
+            uint32_t f = (uint32_t)(L0 / tpc), tt = (uint32_t)(L0 % tpc);  // stepped below
+            for (uint64_t L = L0; L < L1; L++) {
+                if (!mbar_wait(&d_full[db], dph, abort, kWaitBudget)) { record_abort(abort, 7); break; }
+                tc_fence_after();
+                const uint32_t u = (tt * rows_per_k + s_local) / I;
+                const uint32_t lane_addr = tmem + ((32 * q) << 16) + db * (2 * d_cols);
+                float* obase = g.out + ((uint64_t)f * R + k) * g.U + u;
+                constexpr int CH = 16 / kEpiGroups;  // beams per TMEM load (16 or 8)
+                for (uint32_t bc = hw * nbh; bc < (hw + 1) * nbh; bc += CH) {
+                    // Two beams per packed FP32x2 instruction (each lane of the pair rounds
+                    // exactly as the scalar add / multiply / FMA would).
+                    float2 pw2[CH / 2];
+                    float(&pw)[CH] = *reinterpret_cast<float(*)[CH]>(pw2);
+                    if (g.stacked) {
+                        // per polarisation: (hi + lo) re, (hi + lo) im
+    #pragma unroll
+                        for (int j = 0; j < CH; j++) pw[j] = 0.f;
+    #pragma unroll
+                        for (uint32_t p = 0; p < 2; p++) {
+                            uint32_t hr[CH], hi[CH], lr[CH], li[CH];
+                            const uint32_t pa = lane_addr + p * d_cols + bc;
+                            tmem_ld(pa, hr);
+                            tmem_ld(pa + NB, hi);
+                            tmem_ld(pa + 2 * NB, lr);
+                            tmem_ld(pa + 3 * NB, li);
+                            tmem_ld_wait();
+    #pragma unroll
+                            for (int j = 0; j < CH / 2; j++) {
+                                const float2 a = __fadd2_rn(make_float2(__uint_as_float(hr[2 * j]), __uint_as_float(hr[2 * j + 1])),
+                                                            make_float2(__uint_as_float(lr[2 * j]), __uint_as_float(lr[2 * j + 1])));
+                                const float2 b = __fadd2_rn(make_float2(__uint_as_float(hi[2 * j]), __uint_as_float(hi[2 * j + 1])),
+                                                            make_float2(__uint_as_float(li[2 * j]), __uint_as_float(li[2 * j + 1])));
+                                pw2[j] = __ffma2_rn(a, a, __ffma2_rn(b, b, pw2[j]));
+                            }
+                        }
+                    } else {
+                        uint32_t r0[CH], i0[CH], r1[CH], i1[CH];
+                        tmem_ld(lane_addr + bc, r0);
+                        tmem_ld(lane_addr + NB + bc, i0);
+                        tmem_ld(lane_addr + 2 * NB + bc, r1);
+                        tmem_ld(lane_addr + 3 * NB + bc, i1);
                         tmem_ld_wait();
-#pragma unroll
+    #pragma unroll
                         for (int j = 0; j < CH / 2; j++) {
-                            const float2 a = __fadd2_rn(make_float2(__uint_as_float(hr[2 * j]), __uint_as_float(hr[2 * j + 1])),
-                                                        make_float2(__uint_as_float(lr[2 * j]), __uint_as_float(lr[2 * j + 1])));
-                            const float2 b = __fadd2_rn(make_float2(__uint_as_float(hi[2 * j]), __uint_as_float(hi[2 * j + 1])),
-                                                        make_float2(__uint_as_float(li[2 * j]), __uint_as_float(li[2 * j + 1])));
-                            pw2[j] = __ffma2_rn(a, a, __ffma2_rn(b, b, pw2[j]));
+                            const float2 a0 = make_float2(__uint_as_float(r0[2 * j]), __uint_as_float(r0[2 * j + 1]));
+                            const float2 b0 = make_float2(__uint_as_float(i0[2 * j]), __uint_as_float(i0[2 * j + 1]));
+                            const float2 a1 = make_float2(__uint_as_float(r1[2 * j]), __uint_as_float(r1[2 * j + 1]));
+                            const float2 b1 = make_float2(__uint_as_float(i1[2 * j]), __uint_as_float(i1[2 * j + 1]));
+                            pw2[j] = __ffma2_rn(a0, a0, __ffma2_rn(b0, b0, __ffma2_rn(a1, a1, __fmul2_rn(b1, b1))));
                         }
                     }
-                } else {
-                    uint32_t r0[CH], i0[CH], r1[CH], i1[CH];
-                    tmem_ld(lane_addr + bc, r0);
-                    tmem_ld(lane_addr + NB + bc, i0);
-                    tmem_ld(lane_addr + 2 * NB + bc, r1);
-                    tmem_ld(lane_addr + 3 * NB + bc, i1);
-                    tmem_ld_wait();
-#pragma unroll
-                    for (int j = 0; j < CH / 2; j++) {
-                        const float2 a0 = make_float2(__uint_as_float(r0[2 * j]), __uint_as_float(r0[2 * j + 1]));
-                        const float2 b0 = make_float2(__uint_as_float(i0[2 * j]), __uint_as_float(i0[2 * j + 1]));
-                        const float2 a1 = make_float2(__uint_as_float(r1[2 * j]), __uint_as_float(r1[2 * j + 1]));
-                        const float2 b1 = make_float2(__uint_as_float(i1[2 * j]), __uint_as_float(i1[2 * j + 1]));
-                        pw2[j] = __ffma2_rn(a0, a0, __ffma2_rn(b0, b0, __ffma2_rn(a1, a1, __fmul2_rn(b1, b1))));
+                    uint32_t first;
+                    const int cnt = window_reduce<CH, LOGI>(pw, lane, &first);
+    #pragma unroll
+                    for (int j = 0; j < CH; j++) {
+                        if (j < cnt) {
+                            const uint32_t b = bc + first + j;
+                            if (b < g.beams) obase[b * bstride] = pw[j];
+                        }
                     }
                 }
-                uint32_t first;
-                const int cnt = window_reduce<CH, LOGI>(pw, lane, &first);
-#pragma unroll
-                for (int j = 0; j < CH; j++) {
-                    if (j < cnt) {
-                        const uint32_t b = bc + first + j;
-                        if (b < g.beams) obase[b * bstride] = pw[j];
-                    }
-                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&d_empty[db]);
+                if (++db == nacc) { db = 0; dph ^= 1; }
+                if (++tt == tpc) { tt = 0; f++; }
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&d_empty[db]);
-            if (++db == nacc) { db = 0; dph ^= 1; }
-            if (++tt == tpc) { tt = 0; f++; }
         }
     } else if (warp < 2 + kEpiWarps + kConvWarps) {
         // ---------------- operand build ----------------
@@ -1212,7 +1360,7 @@ bool tc_shape(uint64_t B, uint64_t A, TcShape& s, uint64_t T = 0, uint32_t es = 
     s.img_bytes = s.stacked ? (2 * s.KA / 64) * 1024u * s.NB : (s.KA == 64 ? 1536u : 1024u) * s.NB;
     s.raw_bytes = (uint32_t)A * kM * es;
     const size_t op = (2ull * s.KA / 64) * 16384;   // one polarisation's operand
-    // barriers (2 x 8 operand + 2 x 8 raw + 2 x 4 accumulator + 3, 8 bytes each),
+    // barriers (2 x 8 operand + 2 x 8 raw + 3 x 4 accumulator + 4, 8 bytes each),
     // TMEM slot and abort flag, alignment slack
     const size_t fixed = s.img_bytes + 512 + 1024;
     const size_t limit = 227 * 1024;
@@ -1488,6 +1636,10 @@ int tc_run(const char* who, const void* in, const void* plan, void* out, uint64_
         g.total_tiles = (uint64_t)F * (T / kM);
         g.pdl = (pdl && c == 0) ? 1u : 0u;
         g.direct = s.direct;
+        // outputs along TMEM lanes: full 64-beam chunks (separate hi/lo products),
+        // rate 1 CI8, windows of 8 or 16 samples, 16-byte aligned output rows
+        g.transposed = (!s.stacked && s.NB == 64 && rate == 1 && es == 4 && (integration == 8 || integration == 16) &&
+                        U % 4 == 0 && (reinterpret_cast<uintptr_t>(out) & 15u) == 0) ? 1u : 0u;
         // Whole raw stages per CTA (the kernel rounds its share up to raw_tiles); no
         // CTA is left without tiles.
         const uint64_t sms = (uint64_t)sm_count();

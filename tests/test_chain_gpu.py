@@ -36,6 +36,11 @@ CHAINS = [
     ("direct-48-beams", 64, 4, 2048, 48, 1, 16),
     ("direct-two-chunks", 64, 3, 1024, 100, 1, 8),
     ("direct-stacked-32-beams", 64, 4, 1024, 32, 1, 2),
+    # accumulator with outputs along TMEM lanes (full 64-beam chunks, windows of 16):
+    # an odd number of tiles per channel; two chunks with 40 beams in the second and
+    # a 32-antenna K
+    ("lanes-i16", 64, 5, 1152, 64, 1, 16),
+    ("lanes-i16-two-chunks", 24, 3, 2048, 104, 1, 16),
 ]
 
 
