@@ -630,29 +630,37 @@ __device__ __forceinline__ void issue_ka32_t(uint32_t d, uint64_t ad, uint64_t w
 // the output; warps 2 and 3 (the Im rows) keep theirs in registers and add them to
 // the stored partial sums one tile later, once pr_full says those are there.  The
 // Re half signals a tile's partial sums after reading the next tile from TMEM, so
-// neither half waits on the round trip through memory.  The Im half releases an
-// accumulator only after its wait for the previous tile, which keeps the Re half
-// within one phase of it on every pr_full barrier.
+// neither half waits on the round trip through memory.
+//
+// Phases of pr_full: an mbarrier wait tests only the parity of its phase, so the Re
+// half must never complete a barrier's next phase before the Im half has waited
+// for the current one.  Inside the range, the Re half's signal for tile m needs the
+// accumulator of tile m + 1, which needs the Im half's release of tile m + 1 - nacc,
+// which it gives only after its wait for tile m - nacc, the previous phase of the
+// same barrier.  The signal for the range's last tile comes after the loop with no
+// accumulator to gate it, so the Re half first waits for the release of tile
+// n - nacc (that wait of the Im half precedes it).
+//
+// At rate 1 a channel holds tpc tiles of NW outputs and U = tpc NW, so tile L of
+// the chunk's F tpc tiles writes outputs L NW .. L NW + NW - 1 of each beam row.
 template <int LOGI>
 __device__ __forceinline__ void epilogue_transposed(const TcArgs& g, uint32_t tmem, uint32_t d_cols, uint32_t nacc,
                                                     uint64_t* d_full, uint64_t* d_empty, uint64_t* pr_full,
-                                                    volatile int* abort, uint64_t L0, uint64_t L1, uint32_t tpc,
-                                                    uint32_t q, uint32_t lane) {
+                                                    volatile int* abort, uint64_t L0, uint64_t L1, uint32_t q,
+                                                    uint32_t lane) {
     constexpr uint32_t I = 1u << LOGI;
     constexpr int NW = kM / I;                      // windows per tile: 16 or 8
-    constexpr int kCols = LOGI == 3 ? 32 : 64;      // TMEM columns read per wait
+    constexpr int kCols = LOGI == 3 ? 32 : 16;      // TMEM columns read per wait
     const bool re_half = q < 2;
     const uint32_t b = 32u * (q & 1u) + lane;
     const bool valid = b < g.beams;
-    const uint64_t bstride = (uint64_t)g.F * g.U;
+    float* row = g.out + (uint64_t)b * g.F * g.U + L0 * NW;  // this beam's outputs of tile L0
+    const uint32_t n = (uint32_t)(L1 - L0);
     uint32_t db = 0, dph = 0;
-    uint32_t f = (uint32_t)(L0 / tpc), tt = (uint32_t)(L0 % tpc);
-    float* prev = nullptr;       // output row of the previous tile, whose exchange is pending
-    uint32_t pdb = 0, pph = 0;   // its pr_full barrier and parity
-    float pend[NW];              // Im half: the previous tile's own window sums
-    bool ok = true;
-    for (uint64_t L = L0; L < L1; L++) {
-        if (!mbar_wait(&d_full[db], dph, abort, kWaitBudget)) { record_abort(abort, 7); ok = false; break; }
+    float pend[NW];  // Im half: the previous tile's own window sums
+    uint32_t i = 0;
+    for (; i < n; i++) {
+        if (!mbar_wait(&d_full[db], dph, abort, kWaitBudget)) { record_abort(abort, 7); break; }
         tc_fence_after();
         const uint32_t lane_addr = tmem + ((32 * q) << 16) + db * (2 * d_cols);
         float2 acc[NW];
@@ -678,11 +686,13 @@ __device__ __forceinline__ void epilogue_transposed(const TcArgs& g, uint32_t tm
         }
         tc_fence_before();
         __syncwarp();
-        float* o = g.out + (uint64_t)b * bstride + (uint64_t)f * g.U + (uint64_t)tt * NW;
+        // the previous tile's accumulator slot and phase
+        const uint32_t pdb = db ? db - 1 : nacc - 1, pph = db ? dph : dph ^ 1u;
+        float* o = row + (uint64_t)i * NW;
         if (re_half) {
             if (lane == 0) {
                 mbar_arrive(&d_empty[db]);
-                if (prev) mbar_arrive(&pr_full[pdb]);  // stored a tile ago
+                if (i) mbar_arrive(&pr_full[pdb]);  // stored a tile ago
             }
             if (valid) {
 #pragma unroll
@@ -693,36 +703,37 @@ __device__ __forceinline__ void epilogue_transposed(const TcArgs& g, uint32_t tm
             __threadfence_block();  // ordered before lane 0's next arrive on pr_full
             __syncwarp();
         } else {
-            if (prev && !mbar_wait(&pr_full[pdb], pph, abort, kWaitBudget)) { record_abort(abort, 12); ok = false; break; }
+            if (i && !mbar_wait(&pr_full[pdb], pph, abort, kWaitBudget)) { record_abort(abort, 12); break; }
             __syncwarp();
             if (lane == 0) mbar_arrive(&d_empty[db]);
-            if (prev && valid) {
+            if (i && valid) {
 #pragma unroll
                 for (int w = 0; w < NW; w += 4) {
-                    const float4 r = *reinterpret_cast<const float4*>(prev + w);
-                    *reinterpret_cast<float4*>(prev + w) =
+                    const float4 r = *reinterpret_cast<const float4*>(o - NW + w);
+                    *reinterpret_cast<float4*>(o - NW + w) =
                         make_float4(r.x + pend[w], r.y + pend[w + 1], r.z + pend[w + 2], r.w + pend[w + 3]);
                 }
             }
 #pragma unroll
             for (int w = 0; w < NW; w++) pend[w] = acc[w].x + acc[w].y;
         }
-        prev = o;
-        pdb = db;
-        pph = dph;
         if (++db == nacc) { db = 0; dph ^= 1; }
-        if (++tt == tpc) { tt = 0; f++; }
     }
-    if (ok && prev) {
+    if (i == n && n) {
+        // the last tile's exchange (db, dph now name tile n's slot and phase)
+        const uint32_t pdb = db ? db - 1 : nacc - 1, pph = db ? dph : dph ^ 1u;
+        float* o = row + (uint64_t)(n - 1) * NW;
         if (re_half) {
-            if (lane == 0) mbar_arrive(&pr_full[pdb]);
+            // tile n - nacc used this slot in the phase before: wait for its release
+            if (n >= nacc && !mbar_wait(&d_empty[db], dph ^ 1u, abort, kWaitBudget)) record_abort(abort, 13);
+            else if (lane == 0) mbar_arrive(&pr_full[pdb]);
         } else if (mbar_wait(&pr_full[pdb], pph, abort, kWaitBudget)) {
             __syncwarp();
             if (valid) {
 #pragma unroll
                 for (int w = 0; w < NW; w += 4) {
-                    const float4 r = *reinterpret_cast<const float4*>(prev + w);
-                    *reinterpret_cast<float4*>(prev + w) =
+                    const float4 r = *reinterpret_cast<const float4*>(o + w);
+                    *reinterpret_cast<float4*>(o + w) =
                         make_float4(r.x + pend[w], r.y + pend[w + 1], r.z + pend[w + 2], r.w + pend[w + 3]);
                 }
             }
@@ -995,7 +1006,7 @@ __global__ void __launch_bounds__(kThreads, 1) bf_tc_kernel(const TcArgs g, cons
         bool done = false;
         if constexpr (R == 1 && (LOGI == 3 || LOGI == 4) && ES == 4 && kEpiWarps == 4) {
             if (g.transposed) {
-                epilogue_transposed<LOGI>(g, tmem, d_cols, nacc, d_full, d_empty, pr_full, abort, L0, L1, tpc,
+                epilogue_transposed<LOGI>(g, tmem, d_cols, nacc, d_full, d_empty, pr_full, abort, L0, L1,
                                           (uint32_t)(warp & 3), (uint32_t)lane);
                 done = true;
             }

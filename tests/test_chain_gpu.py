@@ -128,6 +128,37 @@ def test_prepare_detect_tc_matches_two_calls(cuda, name, A, F, T, B, R, I):
     assert bl.device_status() == 0
 
 
+@pytest.mark.parametrize("I", [8, 16])
+def test_tensor_core_chain_repeated_launches(cuda, I):
+    # Hundreds of back-to-back launches of a full 64-beam chunk (the accumulator with
+    # outputs along TMEM lanes): every CTA's range ends once per launch, where the
+    # epilogue halves hand the last tile's partial sums over, so an ordering fault
+    # there shows up as an expired bounded wait (a non-zero status word, ~2 s
+    # launches) or as an output that differs from the first launch.
+    A, F, T, B, R = 64, 16, 8192, 64, 1
+    x, w = make(A, F, T, B, 6)
+    lib = _lib.load()
+    xd, wd = dev(x), c64(w)
+    plan = torch.empty(int(lib.blade_beamform_tc_plan_size(B, A, F, 2)), dtype=torch.uint8, device="cuda")
+    call("blade_beamform_tc_prepare", ptr(wd), ptr(plan), B, A, F, 2, stream())
+    outs = [torch.full((B, F * R, T // (R * I), 1), float("nan"), dtype=torch.float32, device="cuda")
+            for _ in range(2)]
+    first = None
+    for k in range(400):
+        o = outs[k % 2]
+        call("blade_beamform_detect_tc", ptr(xd), ptr(plan), ptr(o), B, A, F, T, 2, R, I, stream())
+        if k < 2:
+            torch.cuda.synchronize()
+            if k == 0:
+                first = o.clone()
+        elif k % 50 == 49:
+            assert torch.equal(o, first)
+            assert torch.equal(outs[(k + 1) % 2], first)
+    torch.cuda.synchronize()
+    assert bl.device_status() == 0
+    assert rel_l2(host(first), O.beamform_channelize_detect(x, w, R, I)) < TOL
+
+
 def test_tensor_core_matches_fp32_path(cuda):
     A, F, T, B, R, I = 28, 8, 2048, 16, 4, 4
     x, w = make(A, F, T, B, 3)
