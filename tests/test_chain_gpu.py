@@ -159,6 +159,31 @@ def test_tensor_core_chain_repeated_launches(cuda, I):
     assert rel_l2(host(first), O.beamform_channelize_detect(x, w, R, I)) < TOL
 
 
+@pytest.mark.parametrize("I", [8, 16])
+def test_tensor_core_chain_output_offset_by_one_float(cuda, I):
+    # A full 64-beam chunk with the output 4 bytes past a 16-byte boundary takes the
+    # lane-shuffle epilogue (the lane-major one stores 16-byte vectors); both meet the
+    # FP64 bound and agree with each other.
+    A, F, T, B, R = 64, 3, 2048, 64, 1
+    x, w = make(A, F, T, B, 7)
+    ref = O.beamform_channelize_detect(x, w, R, I)
+    lib = _lib.load()
+    xd, wd = dev(x), c64(w)
+    plan = torch.empty(int(lib.blade_beamform_tc_plan_size(B, A, F, 2)), dtype=torch.uint8, device="cuda")
+    call("blade_beamform_tc_prepare", ptr(wd), ptr(plan), B, A, F, 2, stream())
+    n = B * F * R * (T // (R * I))
+    buf = torch.full((n + 4,), float("nan"), dtype=torch.float32, device="cuda")
+    aligned, offset = buf[:n], buf[1:n + 1]
+    assert aligned.data_ptr() % 16 == 0 and offset.data_ptr() % 16 == 4
+    call("blade_beamform_detect_tc", ptr(xd), ptr(plan), ptr(offset), B, A, F, T, 2, R, I, stream())
+    y_off = host(offset).reshape(ref.shape)
+    call("blade_beamform_detect_tc", ptr(xd), ptr(plan), ptr(aligned), B, A, F, T, 2, R, I, stream())
+    y_al = host(aligned).reshape(ref.shape)
+    assert bl.device_status() == 0
+    assert rel_l2(y_off, ref) < TOL and rel_l2(y_al, ref) < TOL
+    assert rel_l2(y_off, y_al) < 1e-6
+
+
 def test_tensor_core_matches_fp32_path(cuda):
     A, F, T, B, R, I = 28, 8, 2048, 16, 4, 4
     x, w = make(A, F, T, B, 3)
