@@ -220,7 +220,9 @@ BLADE_API int blade_beamform_detect_f32(int in_type, const void* in, const void*
  * out F32 [B, F*rate, T/rate/I, 1].
  * Limits (blade_beamform_detect_tc_supported() returns 1 when met): P = 2,
  * 1 <= A <= 64, any B (64 beams per pass), T % 128 == 0, rate in {1, 2, 4},
- * I a power of two <= 32.  Input and plan 16-byte aligned.
+ * I a power of two <= 32.  Input and plan 16-byte aligned, output 4-byte
+ * aligned; at rate 1 with I = 8 or 16, a 16-byte aligned output lets each full
+ * 64-beam pass use the faster epilogue (outputs agree within FP32 rounding).
  * Composes the same reference stages as blade_beamform_detect_f32.
  * ------------------------------------------------------------------------- */
 BLADE_API uint64_t blade_beamform_tc_plan_size(uint64_t B, uint64_t A, uint64_t F, uint64_t P);
