@@ -1351,6 +1351,70 @@ __global__ void __launch_bounds__(256) tc_prepare_kernel(const float2* __restric
     }
 }
 
+// The same split for KA = 64 images without stacking (more than 32 beams per
+// chunk), through shared memory: a CTA takes 8 beams x 4 channels x both
+// polarisations of one chunk.  It reads each (beam, antenna) row's 4 x 2 phasors
+// as one 64-byte run, and each warp then writes 4 whole 128-byte image rows per
+// block (lanes: 8 antenna groups x 4 beams), where the one-thread-per-chunk form
+// writes 32 chunks into 32 different channels' images.  Same arithmetic per
+// element, so the image is bit-identical.
+constexpr uint32_t kPrepBeams = 8, kPrepChans = 4, kPrepPad = 10;  // float2 per 8-antenna group (8 + 2 pad)
+__global__ void __launch_bounds__(256) tc_prepare_wide_kernel(const float2* __restrict__ ph, uint8_t* __restrict__ plan,
+                                                              uint32_t B, uint32_t A, uint32_t F, uint32_t NB,
+                                                              uint32_t img_bytes) {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    // [beam][channel][pol][antenna group][8 antennas + pad]: a task's 8 phasors are
+    // contiguous, and the 80-byte group pitch keeps a quarter-warp's 16-byte reads
+    // (8 groups) on distinct banks
+    __shared__ __align__(16) float2 sp[kPrepBeams][kPrepChans][2][8][kPrepPad];
+    const uint32_t f0 = blockIdx.x * kPrepChans, nb0 = blockIdx.y * kPrepBeams, c = blockIdx.z;
+    // load: element q = (bl, a, col), col = 2 fl + p fastest (the phasors' own order)
+#pragma unroll 4
+    for (uint32_t q = threadIdx.x; q < kPrepBeams * 64 * 2 * kPrepChans; q += blockDim.x) {
+        const uint32_t col = q & 7u, a = (q >> 3) & 63u, bl = q >> 9;
+        const uint32_t fl = col >> 1, pp = col & 1u;
+        const uint32_t b = c * kMaxNB + nb0 + bl;
+        float2 w = make_float2(0.f, 0.f);
+        if (b < B && a < A && f0 + fl < F) w = ph[((uint64_t)(b * (uint64_t)A + a) * F + f0 + fl) * 2 + pp];
+        sp[bl][fl][pp][a >> 3][a & 7u] = w;
+    }
+    __syncthreads();
+    const uint32_t ph_bytes = 3u * NB * 128u;
+    // tasks t = (j, bl, p, fl), j fastest: a warp covers 8 groups x 4 beams
+    for (uint32_t t = threadIdx.x; t < kPrepBeams * 8 * 2 * kPrepChans; t += blockDim.x) {
+        const uint32_t j = t & 7u, bl = (t >> 3) & 7u, pp = (t >> 6) & 1u, fl = t >> 7;
+        const uint32_t f = f0 + fl;
+        if (f >= F) continue;
+        __half rh[8], ih[8], rl[8], il[8], nih[8], nil[8];
+        const float4* src = reinterpret_cast<const float4*>(&sp[bl][fl][pp][j][0]);
+#pragma unroll
+        for (int e2 = 0; e2 < 4; e2++) {
+            const float4 v = src[e2];
+            const float wr[2] = {v.x, v.z}, wi[2] = {v.y, v.w};
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int e = 2 * e2 + u;
+                rh[e] = __float2half_rn(wr[u]);
+                ih[e] = __float2half_rn(wi[u]);
+                rl[e] = __float2half_rn(wr[u] - __half2float(rh[e]));
+                il[e] = __float2half_rn(wi[u] - __half2float(ih[e]));
+                nih[e] = __hneg(ih[e]);
+                nil[e] = __hneg(il[e]);
+            }
+        }
+        const uint32_t nb = nb0 + bl, k0 = j * 8;
+        uint8_t* base = plan + ((uint64_t)c * F + f) * img_bytes + (uint64_t)pp * 2 * ph_bytes;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            uint8_t* blk = base + h * ph_bytes;
+            // three blocks of NB rows x 64 K: [-Wi | Wr | Wi]
+            put_chunk(blk, NB, nb, k0, pack8(h ? nil : nih));
+            put_chunk(blk + NB * 128u, NB, nb, k0, pack8(h ? rl : rh));
+            put_chunk(blk + 2u * NB * 128u, NB, nb, k0, pack8(h ? il : ih));
+        }
+    }
+}
+
 struct TcShape {
     uint32_t NB, KA, nchunks, img_bytes, raw_bytes, a_stages, r_stages, stacked;
     uint32_t raw_tiles, raw_row, direct;
@@ -1588,9 +1652,16 @@ extern "C" int blade_beamform_tc_prepare(const void* phasors, void* plan, uint64
     if (!aligned16(plan)) return set_error(BLADE_ERROR, "blade_beamform_tc_prepare: plan must be 16-byte aligned");
     const uint64_t n = (uint64_t)s.nchunks * F * 2 * s.NB * (s.KA / 8);
     if (n > 0xFFFFFFFFull) return set_error(BLADE_ERROR, "blade_beamform_tc_prepare: too many channels");
-    tc_prepare_kernel<<<grid_for(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-        static_cast<const float2*>(phasors), static_cast<uint8_t*>(plan), (uint32_t)B, (uint32_t)A, (uint32_t)F,
-        s.NB, s.KA, s.nchunks, s.img_bytes, s.stacked);
+    if (!s.stacked && s.KA == 64) {
+        const dim3 grid((unsigned)((F + kPrepChans - 1) / kPrepChans), s.NB / kPrepBeams, s.nchunks);
+        tc_prepare_wide_kernel<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+            static_cast<const float2*>(phasors), static_cast<uint8_t*>(plan), (uint32_t)B, (uint32_t)A, (uint32_t)F,
+            s.NB, s.img_bytes);
+    } else {
+        tc_prepare_kernel<<<grid_for(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+            static_cast<const float2*>(phasors), static_cast<uint8_t*>(plan), (uint32_t)B, (uint32_t)A, (uint32_t)F,
+            s.NB, s.KA, s.nchunks, s.img_bytes, s.stacked);
+    }
     return check_launch("blade_beamform_tc_prepare");
 }
 
