@@ -1352,13 +1352,14 @@ __global__ void __launch_bounds__(256) tc_prepare_kernel(const float2* __restric
 }
 
 // The same split for KA = 64 images without stacking (more than 32 beams per
-// chunk), through shared memory: a CTA takes 8 beams x 4 channels x both
-// polarisations of one chunk.  It reads each (beam, antenna) row's 4 x 2 phasors
-// as one 64-byte run, and each warp then writes 4 whole 128-byte image rows per
+// chunk), through shared memory: a CTA takes 8 beams x 2 channels x both
+// polarisations of one chunk (20 KB of shared memory; the dense block's 1024
+// CTAs are resident at once).  It reads each (beam, antenna) row's 2 x 2 phasors
+// as one 32-byte run, and each warp then writes 4 whole 128-byte image rows per
 // block (lanes: 8 antenna groups x 4 beams), where the one-thread-per-chunk form
 // writes 32 chunks into 32 different channels' images.  Same arithmetic per
 // element, so the image is bit-identical.
-constexpr uint32_t kPrepBeams = 8, kPrepChans = 4, kPrepPad = 10;  // float2 per 8-antenna group (8 + 2 pad)
+constexpr uint32_t kPrepBeams = 8, kPrepChans = 2, kPrepPad = 10;  // float2 per 8-antenna group (8 + 2 pad)
 __global__ void __launch_bounds__(256) tc_prepare_wide_kernel(const float2* __restrict__ ph, uint8_t* __restrict__ plan,
                                                               uint32_t B, uint32_t A, uint32_t F, uint32_t NB,
                                                               uint32_t img_bytes) {
@@ -1369,9 +1370,10 @@ __global__ void __launch_bounds__(256) tc_prepare_wide_kernel(const float2* __re
     __shared__ __align__(16) float2 sp[kPrepBeams][kPrepChans][2][8][kPrepPad];
     const uint32_t f0 = blockIdx.x * kPrepChans, nb0 = blockIdx.y * kPrepBeams, c = blockIdx.z;
     // load: element q = (bl, a, col), col = 2 fl + p fastest (the phasors' own order)
+    constexpr uint32_t kCol = 2 * kPrepChans;
 #pragma unroll 4
-    for (uint32_t q = threadIdx.x; q < kPrepBeams * 64 * 2 * kPrepChans; q += blockDim.x) {
-        const uint32_t col = q & 7u, a = (q >> 3) & 63u, bl = q >> 9;
+    for (uint32_t q = threadIdx.x; q < kPrepBeams * 64 * kCol; q += blockDim.x) {
+        const uint32_t col = q % kCol, a = (q / kCol) % 64u, bl = q / (64u * kCol);
         const uint32_t fl = col >> 1, pp = col & 1u;
         const uint32_t b = c * kMaxNB + nb0 + bl;
         float2 w = make_float2(0.f, 0.f);
@@ -1382,7 +1384,8 @@ __global__ void __launch_bounds__(256) tc_prepare_wide_kernel(const float2* __re
     const uint32_t ph_bytes = 3u * NB * 128u;
     // tasks t = (j, bl, p, fl), j fastest: a warp covers 8 groups x 4 beams
     for (uint32_t t = threadIdx.x; t < kPrepBeams * 8 * 2 * kPrepChans; t += blockDim.x) {
-        const uint32_t j = t & 7u, bl = (t >> 3) & 7u, pp = (t >> 6) & 1u, fl = t >> 7;
+        const uint32_t j = t & 7u, bl = (t / 8u) % kPrepBeams, pp = (t / (8u * kPrepBeams)) & 1u,
+                       fl = t / (16u * kPrepBeams);
         const uint32_t f = f0 + fl;
         if (f >= F) continue;
         __half rh[8], ih[8], rl[8], il[8], nih[8], nil[8];
